@@ -1,0 +1,337 @@
+#!/usr/bin/env python
+"""getrates throughput on B200: Mpoints/s of the 53-species / 325-reaction
+workload (2^20 points per GPU), one JSON line on rank 0.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one getrates pass over the GPU's 2^20 points (inputs resident in
+HBM; Y alone is 445 MB, larger than the 126 MB L2, so no flush is needed).
+`value` is the headline form -- the fastest arithmetic mode whose error
+against the FP64 oracle meets 1e-6 (normwise) -- and the FP64 kernel is
+reported beside it.  Under torchrun every rank runs its own 2^20 points
+(weak scaling, no collective on the data path); times are the max over
+ranks.  `--impl reference` times the FP64 CPU restatement of the reference's
+generated getrates on all host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "getrates Mpoints/s on 1 B200: mixed/surrogate vs FP64 kernel at ≤1e-6 rel err"
+WORKLOAD = "synthetic mechanism, 53 species / 325 reactions (28 three-body, 29 Troe, ~70% reversible), 2^20 points per GPU"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--ng", type=int, default=1 << 20)
+    ap.add_argument("--modes", default="fp64,mixed")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    """SM clock and throttle reasons sampled every ~5 ms through NVML while running."""
+
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            idx = device
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            if vis:
+                ids = [v.strip() for v in vis.split(",") if v.strip()]
+                if device < len(ids) and ids[device].isdigit():
+                    idx = int(ids[device])
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+            self._nv = pynvml
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self._nv = None
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for name, bit in self.REASONS.items():
+                    if mask & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.005)
+
+    def __enter__(self):
+        if self._nv is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t is not None:
+            self._t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": 0}
+        return {"sm_mhz": float(statistics.median(self.samples)), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def ncu_traffic(mode: str, ns: int, nr: int):
+    """DRAM bytes per point of the getrates kernel from the committed ncu summary."""
+    path = os.path.join(REPO, "profiles", "getrates_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        p = line.split()
+        if len(p) == 4 and not line.startswith("#") and p[0] == mode and int(p[1]) == ns and int(p[2]) == nr:
+            return float(p[3])
+    return None
+
+
+# ------------------------------------------------------------ reference arm
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from chemgen_b200 import pack, synthetic
+    from oracle import oracle
+    mech = synthetic.gri_shape()
+    blob = pack.pack(mech).to_blob()
+    cores = os.cpu_count() or 1
+    P, T, Y = synthetic.states(mech.ns, 4096, seed=1000)
+    t0 = time.perf_counter()
+    oracle.getrates(blob, P[:512], T[:512], Y[:, :512].copy(), nthreads=cores)
+    pilot = 512 / (time.perf_counter() - t0)
+    sample = int(min(args.ng, max(1024, pilot * 2.0)))
+    P, T, Y = synthetic.states(mech.ns, sample, seed=1000)
+    for _ in range(max(args.warmup, 0)):
+        oracle.getrates(blob, P, T, Y, nthreads=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.getrates(blob, P, T, Y, nthreads=cores)
+    dt = (time.perf_counter() - t0) / max(args.steps, 1)
+    value = sample / dt / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mpoints/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "mechanism": mech.name, "points_per_step": sample},
+            "cpu_baseline": {"value": value, "unit": "Mpoints/s", "cores": cores, "kind": "port",
+                             "sample": f"{sample} points of the workload per step (FP64 C restatement of the "
+                                       f"reference's generated getrates, OpenMP over points)"},
+            "e2e": {"value": value, "unit": "Mpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def time_steps(fn, steps, warmup, stream):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / max(steps, 1)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from chemgen_b200 import ops, pack, synthetic
+    from chemgen_b200.runtime import GpuMechanism, lib
+    import ctypes
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    mech = synthetic.gri_shape()
+    blob = pack.pack(mech).to_blob()
+    gm = GpuMechanism(blob, device=local_rank)
+    ng = args.ng
+    P, T, Y = synthetic.states(mech.ns, ng, seed=1000 + rank)
+    Pd, Td, Yd = (torch.from_numpy(x).to(dev) for x in (P, T, Y))
+    W = torch.empty_like(Yd)
+    stream = torch.cuda.current_stream()
+
+    modes = []
+    for m in args.modes.split(","):
+        try:
+            gm.getrates(Pd[:64].contiguous(), Td[:64].contiguous(), Yd[:, :64].contiguous(), mode=m)
+            modes.append(m)
+        except Exception:
+            pass
+    torch.cuda.synchronize()
+
+    # FP64 roofline denominators, measured on this GPU
+    fma_tf, c_exp, c_log, c_rcp = (ctypes.c_double() for _ in range(4))
+    lib().chemgen_probe_fp64(local_rank, ctypes.byref(fma_tf), ctypes.byref(c_exp), ctypes.byref(c_log),
+                             ctypes.byref(c_rcp))
+    inv = ops.inventory(mech)
+    flop_pt = ops.flop_equivalents(inv, c_exp.value, c_log.value, c_rcp.value)
+    bytes_pt = ops.bytes_per_point(mech.ns)
+    hbm_peak, hbm_src = measured_peaks()
+
+    results = {}
+    for m in modes:
+        fn = lambda m=m: gm.getrates(Pd, Td, Yd, out=W, mode=m, stream=stream)
+        ms = time_steps(fn, args.steps, args.warmup, stream)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        results[m] = {"ms_per_step": ms, "value": ng * world / (ms * 1e-3) / 1e6}
+
+    # errors and CPU baseline on a bounded sample (rank 0, single GPU)
+    err = {}
+    cpu = None
+    if rank == 0 and world == 1:
+        from oracle import oracle
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        oracle.getrates(blob, P[:512], T[:512], np.ascontiguousarray(Y[:, :512]), nthreads=cores)
+        pilot = 512 / (time.perf_counter() - t0)
+        sample = int(min(ng, max(2048, pilot * args.cpu_seconds)))
+        idx = np.sort(np.random.default_rng(7).choice(ng, sample, replace=False))
+        Ps, Ts, Ys = P[idx], T[idx], np.ascontiguousarray(Y[:, idx])
+        t0 = time.perf_counter()
+        r = oracle.rates(blob, Ps, Ts, Ys, mech.nr, nthreads=cores) if sample <= 65536 else None
+        t_rates = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        w_ref = oracle.getrates(blob, Ps, Ts, Ys, nthreads=cores)
+        dt = time.perf_counter() - t0
+        cpu = {"value": sample / dt / 1e6, "unit": "Mpoints/s", "cores": cores, "kind": "port",
+               "sample": f"{sample} random points of the workload, FP64 C restatement of the reference's "
+                         f"generated getrates, OpenMP over points ({dt:.1f} s)"}
+        idx_t = torch.from_numpy(idx).to(dev)
+        for m in modes:
+            gm.getrates(Pd, Td, Yd, out=W, mode=m, stream=stream)
+            w = W.index_select(1, idx_t).cpu().numpy()
+            S = r["S"] if r is not None else None
+            err[m] = oracle.errors(w, w_ref, S)
+        del t_rates
+
+    ok = [m for m in modes if m in err and err[m]["norm_max"] <= 1e-6] or modes[:1]
+    head = max(ok, key=lambda m: results[m]["value"])
+
+    # clocks during a timed pass of the headline mode
+    sampler = ClockSampler(local_rank)
+    fn = lambda: gm.getrates(Pd, Td, Yd, out=W, mode=head, stream=stream)
+    steps_c = max(args.steps, int(math.ceil(1500.0 / max(results[head]["ms_per_step"], 1e-3))))
+    with sampler:
+        ms_c = time_steps(fn, steps_c, 2, stream)
+    clocks = sampler.summary()
+    clocks["timed_ms_per_step"] = ms_c
+
+    # end to end through the host-pointer API: pinned inputs in, wdot back on the host
+    Ph, Th, Yh = (torch.from_numpy(x).pin_memory() for x in (P, T, Y))
+    Wh = torch.empty_like(Yh).pin_memory()
+    for _ in range(2):
+        gm.getrates_host(Ph, Th, Yh, out=Wh.numpy(), mode=head)
+    k_e2e = max(3, min(args.steps, 50))
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(k_e2e):
+        gm.getrates_host(Ph, Th, Yh, out=Wh.numpy(), mode=head)
+    e2e_s = (time.perf_counter() - t0) / k_e2e
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    if rank != 0:
+        return
+    def roof(m):
+        ms = results[m]["ms_per_step"]
+        achieved = flop_pt * ng / (ms * 1e-3) / 1e12
+        return {"bound": "fp64", "achieved": achieved, "peak": fma_tf.value, "unit": "TFLOP/s",
+                "frac": achieved / fma_tf.value,
+                "traffic": (lambda b: None if b is None else b * ng)(ncu_traffic(m, mech.ns, mech.nr)),
+                "peak_source": "FP64 FMA rate measured live on this GPU (chemgen_probe_fp64)",
+                "flop_equiv_per_point": flop_pt,
+                "transcendental_cost_fma": {"exp": c_exp.value, "log": c_log.value, "rcp": c_rcp.value},
+                "hbm": {"achieved_gbs": bytes_pt * ng / (ms * 1e-3) / 1e9, "peak_gbs": hbm_peak,
+                        "frac": bytes_pt * ng / (ms * 1e-3) / 1e9 / hbm_peak, "peak_source": hbm_src,
+                        "bytes_per_point": bytes_pt}}
+    line = {"metric": METRIC, "value": results[head]["value"], "unit": "Mpoints/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": results[head]["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if head == "fp64" else "f32+f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "mechanism": mech.name, "points_per_gpu": ng, "mode": head,
+                       "l2": "inputs larger than L2 (Y is 445 MB per GPU per step)"},
+            "roofline": roof(head),
+            "cpu_baseline": cpu,
+            "e2e": {"value": ng * world / e2e_s / 1e6, "unit": "Mpoints/s",
+                    "h2d_bytes_per_step": (2 + mech.ns) * ng * 8, "d2h_bytes_per_step": mech.ns * ng * 8,
+                    "api": "chemgen_getrates_host (pinned host buffers, 2-stream chunked copies)"},
+            "gpu_launches": args.steps,
+            "clocks": clocks,
+            "modes": {m: dict(results[m], err=err.get(m), roofline=roof(m)) for m in modes}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

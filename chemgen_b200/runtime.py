@@ -1,0 +1,170 @@
+"""Python side of the C ABI (include/chemgen_b200.h), through ctypes.
+
+PyTorch provides device memory and streams; every computation is a call into
+libchemgen_b200.so.  There is no CPU fallback: when the library is missing or
+cannot be loaded, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Union
+
+import numpy as np
+
+from .mechanism import Mechanism
+from .pack import pack
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libchemgen_b200.so")
+
+MODES = {"fp64": 0, "mixed": 1}
+STATUS = {0: "ok", 1: "invalid argument", 2: "mechanism blob rejected", 3: "CUDA error",
+          4: "out of device memory", 5: "pointer not 8-byte aligned", 6: "mechanism not supported by this path",
+          7: "size exceeds a fixed capacity", 8: "no process-wide mechanism installed"}
+
+
+class ChemgenError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS.get(status, 'unknown status')} (status {status})")
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded CUDA library; raises if it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m chemgen_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i64, sz, ci = ctypes.c_void_p, ctypes.c_int64, ctypes.c_size_t, ctypes.c_int
+    L.chemgen_version.restype = ctypes.c_char_p
+    L.chemgen_status_string.restype = ctypes.c_char_p
+    L.chemgen_status_string.argtypes = [ci]
+    L.chemgen_create.argtypes = [vp, sz, ci, ctypes.POINTER(vp)]
+    L.chemgen_destroy.argtypes = [vp]
+    L.chemgen_num_species.argtypes = [vp]
+    L.chemgen_num_reactions.argtypes = [vp]
+    L.chemgen_getrates.argtypes = [vp, vp, vp, i64, vp, vp, vp]
+    L.chemgen_getrates_ex.argtypes = [vp, ci, vp, vp, i64, vp, vp, vp]
+    L.chemgen_workspace_bytes.argtypes = [vp, ci, i64, ctypes.POINTER(sz)]
+    L.chemgen_getrates_ws.argtypes = [vp, ci, vp, vp, i64, vp, vp, vp, sz, vp]
+    L.chemgen_getrates_host.argtypes = [vp, ci, vp, vp, i64, vp, vp]
+    L.chemgen_init_constants.argtypes = [vp, sz]
+    L.chemgen_free_constants.argtypes = []
+    L.getrates_hip_wrapper_v1.argtypes = [vp, vp, ci, vp, vp, vp, vp]
+    L.getrates_hip_wrapper_v1.restype = None
+    L.chemgen_last_wrapper_status.argtypes = []
+    for f in ("chemgen_create", "chemgen_destroy", "chemgen_num_species", "chemgen_num_reactions",
+              "chemgen_getrates", "chemgen_getrates_ex", "chemgen_workspace_bytes", "chemgen_getrates_ws",
+              "chemgen_getrates_host", "chemgen_init_constants", "chemgen_free_constants",
+              "chemgen_last_wrapper_status"):
+        getattr(L, f).restype = ci
+    _lib = L
+    return L
+
+
+def check(status: int, what: str) -> None:
+    if status != 0:
+        raise ChemgenError(status, what)
+
+
+def _ptr(t) -> int:
+    if t is None:
+        return 0
+    if isinstance(t, int):
+        return t
+    if isinstance(t, np.ndarray):
+        return t.ctypes.data
+    return t.data_ptr()
+
+
+def _stream(stream) -> int:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+class GpuMechanism:
+    """A mechanism loaded on one GPU (one chemgen_handle)."""
+
+    def __init__(self, mech: Union[Mechanism, bytes], device: int = 0):
+        self.blob = mech if isinstance(mech, (bytes, bytearray)) else pack(mech).to_blob()
+        self.mech = None if isinstance(mech, (bytes, bytearray)) else mech
+        self.device = device
+        self._buf = ctypes.create_string_buffer(bytes(self.blob), len(self.blob))
+        h = ctypes.c_void_p()
+        check(lib().chemgen_create(self._buf, len(self.blob), device, ctypes.byref(h)), "chemgen_create")
+        self._h = h
+        self.ns = lib().chemgen_num_species(h)
+        self.nr = lib().chemgen_num_reactions(h)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().chemgen_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def workspace_bytes(self, ng: int, mode: str = "fp64") -> int:
+        out = ctypes.c_size_t()
+        check(lib().chemgen_workspace_bytes(self._h, MODES[mode], ng, ctypes.byref(out)), "chemgen_workspace_bytes")
+        return out.value
+
+    def getrates_ptr(self, P: int, T: int, ng: int, Y: int, wdot: int, mode: str = "fp64", stream=None) -> None:
+        """Raw device pointers (species-major Y/wdot)."""
+        check(lib().chemgen_getrates_ex(self._h, MODES[mode], P, T, ng, Y, wdot, _stream(stream)),
+              "chemgen_getrates_ex")
+
+    def getrates(self, P, T, Y, out=None, mode: str = "fp64", stream=None):
+        """torch CUDA float64 tensors: P[ng], T[ng], Y[ns, ng] -> wdot[ns, ng]."""
+        import torch
+        ns, ng = Y.shape
+        if ns != self.ns:
+            raise ValueError(f"Y has {ns} species, the mechanism {self.ns}")
+        for name, t in (("P", P), ("T", T), ("Y", Y)):
+            if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+                raise ValueError(f"{name} must be a contiguous float64 CUDA tensor")
+        if P.numel() != ng or T.numel() != ng:
+            raise ValueError("P and T must have ng entries")
+        if out is None:
+            out = torch.empty_like(Y)
+        self.getrates_ptr(P.data_ptr(), T.data_ptr(), ng, Y.data_ptr(), out.data_ptr(), mode, stream)
+        return out
+
+    def getrates_ws(self, P, T, Y, out, workspace, mode: str = "fp64", stream=None):
+        ns, ng = Y.shape
+        wb = workspace.numel() * workspace.element_size() if workspace is not None else 0
+        check(lib().chemgen_getrates_ws(self._h, MODES[mode], P.data_ptr(), T.data_ptr(), ng, Y.data_ptr(),
+                                        out.data_ptr(), _ptr(workspace), wb, _stream(stream)),
+              "chemgen_getrates_ws")
+        return out
+
+    def getrates_host(self, P: np.ndarray, T: np.ndarray, Y: np.ndarray, out: Optional[np.ndarray] = None,
+                      mode: str = "fp64") -> np.ndarray:
+        """Host (numpy or pinned torch CPU) arrays in, host wdot out."""
+        ns, ng = Y.shape
+        if out is None:
+            out = np.empty((ns, ng))
+        check(lib().chemgen_getrates_host(self._h, MODES[mode], _ptr(P), _ptr(T), ng, _ptr(Y), _ptr(out)),
+              "chemgen_getrates_host")
+        return out
+
+
+def version() -> str:
+    return lib().chemgen_version().decode()

@@ -1,0 +1,107 @@
+/*
+ * chemgen_b200: C ABI of the B200 getrates library (libchemgen_b200.so).
+ *
+ * getrates(P, T, Y) -> wdot: net molar production rate of every species at
+ * every grid point, in the reference's units and layout:
+ *   P     dyne/cm^2, double[ng]
+ *   T     K,         double[ng]
+ *   Y     mass fractions, double[ns*ng], species-major: Y[k*ng + i]
+ *   wdot  mol/(cm^3 s),   double[ns*ng], same layout
+ * (reference: chemgen/templates/reactions_hip/hip_v1_h.j2:7-13 and
+ *  chemgen/templates/reactions_hip/device_functions_h.j2:701-719).
+ *
+ * Every call returns a chemgen_status; nothing here exits the process or
+ * prints (the reference's HIP wrappers print and return, constants.py:7-24,
+ * and its rocBLAS path exits, reactions_hip/hip_v4_h.j2:12-23).
+ * Device-pointer calls are asynchronous on the given stream (NULL = the
+ * legacy default stream); host-pointer calls return when wdot is on the host.
+ */
+#ifndef CHEMGEN_B200_H
+#define CHEMGEN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum chemgen_status {
+    CHEMGEN_OK = 0,
+    CHEMGEN_ERR_INVALID_ARGUMENT = 1,   /* NULL handle/pointer, ng < 0, bad mode */
+    CHEMGEN_ERR_BAD_MECHANISM = 2,      /* blob rejected by the parser */
+    CHEMGEN_ERR_CUDA = 3,               /* a CUDA runtime call failed */
+    CHEMGEN_ERR_OUT_OF_MEMORY = 4,
+    CHEMGEN_ERR_MISALIGNED = 5,         /* a device pointer is not 8-byte aligned */
+    CHEMGEN_ERR_UNSUPPORTED = 6,        /* mechanism outside what a path supports */
+    CHEMGEN_ERR_TOO_LARGE = 7,          /* ng beyond a fixed capacity */
+    CHEMGEN_ERR_NO_GLOBAL_MECHANISM = 8 /* drop-in wrapper called before chemgen_init_constants */
+} chemgen_status;
+
+/* Arithmetic modes of chemgen_getrates_ex. */
+typedef enum chemgen_mode {
+    CHEMGEN_MODE_FP64 = 0,              /* plain FP64, the reference's arithmetic */
+    CHEMGEN_MODE_MIXED = 1              /* FP32 rate math, FP64 Gibbs/Kc exponents and wdot sums */
+} chemgen_mode;
+
+typedef struct chemgen_handle chemgen_handle;
+
+const char* chemgen_version(void);
+const char* chemgen_status_string(int status);
+
+/* Load a packed mechanism (chemgen_b200/pack.py) onto `device`.
+ * Replaces: copyConstantsToDevice (chemgen/constants.py:119-240) and
+ * init_chemgen's allocations (chemgen/templates/chemgen_mod.j2:108-137).
+ * Unlike the reference's __constant__ symbols, any number of handles coexist. */
+int chemgen_create(const void* blob, size_t nbytes, int device, chemgen_handle** out);
+int chemgen_destroy(chemgen_handle* h);
+int chemgen_num_species(const chemgen_handle* h);
+int chemgen_num_reactions(const chemgen_handle* h);
+
+/* FP64 getrates on device pointers.
+ * Replaces: getrates_hip_wrapper_v1..v4 (reactions_hip/hip_v1_cpp.j2:339-372,
+ * hip_v2_cpp.j2:1078-1160) and the generated getrates (python_header.j2:25).
+ * Any ng >= 0 (the reference requires ng to be a multiple of its block). */
+int chemgen_getrates(chemgen_handle* h, const double* P, const double* T, int64_t ng, const double* Y,
+                     double* wdot, void* stream);
+
+/* Same with an explicit arithmetic mode. */
+int chemgen_getrates_ex(chemgen_handle* h, int mode, const double* P, const double* T, int64_t ng,
+                        const double* Y, double* wdot, void* stream);
+
+/* Scratch a call needs for `ng` points in `mode` (0 when the per-point state
+ * fits in shared memory), and the variant that uses caller-owned scratch of
+ * at least that many bytes (256-byte aligned) instead of library-owned memory. */
+int chemgen_workspace_bytes(const chemgen_handle* h, int mode, int64_t ng, size_t* bytes);
+int chemgen_getrates_ws(chemgen_handle* h, int mode, const double* P, const double* T, int64_t ng,
+                        const double* Y, double* wdot, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Host-pointer getrates: copies P, T, Y to the device, computes, copies wdot
+ * back, and returns when wdot is on the host.  The copies of one chunk of
+ * points overlap the kernels of the previous chunk (two streams).  Pinned
+ * host memory gives the fastest copies; pageable memory works.
+ * Replaces: chemgen_m::getrates_gpu (chemgen/templates/chemgen_mod.j2:139-166),
+ * which maps host arrays with OpenMP target data. */
+int chemgen_getrates_host(chemgen_handle* h, int mode, const double* P, const double* T, int64_t ng,
+                          const double* Y, double* wdot);
+
+/* Drop-in for the reference's process-global API.
+ * chemgen_init_constants replaces copyConstantsToDevice
+ * (chemgen/constants.py:119-240): it installs one process-wide mechanism.
+ * getrates_hip_wrapper_v1 has the exact signature of the reference's wrapper
+ * (reactions_hip/hip_v1_h.j2:7-13): device pointers, ng points, Y/wdot
+ * species-major, log_eg and log_c caller-owned scratch of ng*ns doubles each
+ * (used here as the per-point state when the mechanism is too large for
+ * shared memory), synchronous on the default stream.  It returns void like
+ * the reference; chemgen_last_wrapper_status() reports the outcome. */
+int chemgen_init_constants(const void* blob, size_t nbytes);
+int chemgen_free_constants(void);
+void getrates_hip_wrapper_v1(double* P, double* Temp, int ng, double* Ysp, double* wdot, double* log_eg,
+                             double* log_c);
+int chemgen_last_wrapper_status(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHEMGEN_B200_H */

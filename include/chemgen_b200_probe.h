@@ -1,0 +1,19 @@
+/*
+ * Measurement helpers of libchemgen_b200.so (no counterpart in the
+ * reference, whose timing is a Fortran cpu_time around one call,
+ * chemgen/templates/chemistry_mini_app.j2:73-99).
+ *
+ * chemgen_probe_fp64: FP64 FMA throughput of `device` (TFLOP/s, 2 flops per
+ * FMA) and the throughput cost of one exp, log and Newton-refined reciprocal
+ * as used by the kernels, in FP64-FMA equivalents.  Returns 0 on success.
+ */
+#ifndef CHEMGEN_B200_PROBE_H
+#define CHEMGEN_B200_PROBE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+int chemgen_probe_fp64(int device, double* fma_tflops, double* exp_fma, double* log_fma, double* rcp_fma);
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,165 @@
+"""CUDA getrates against the oracle and the reference's generated code, all
+through the C ABI.  FP64 bar: normwise error <= 1e-10 (max over points of
+max_k |dw_k| / max_k |w_k|) and gross-scaled error <= 1e-10."""
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden
+from chemgen_b200 import pack, synthetic
+from chemgen_b200.runtime import GpuMechanism
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+TOL_FP64 = 1e-10
+
+
+def _run(gm, P, T, Y, mode="fp64"):
+    import torch
+    dev = torch.device("cuda", gm.device)
+    Pt = torch.from_numpy(np.ascontiguousarray(P)).to(dev)
+    Tt = torch.from_numpy(np.ascontiguousarray(T)).to(dev)
+    Yt = torch.from_numpy(np.ascontiguousarray(Y)).to(dev)
+    w = gm.getrates(Pt, Tt, Yt, mode=mode)
+    torch.cuda.synchronize()
+    return w.cpu().numpy()
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_fp64_matches_reference_golden(name):
+    mech, d = load_golden(name)
+    blob = pack.pack(mech).to_blob()
+    gm = GpuMechanism(blob)
+    w = _run(gm, d["P"], d["T"], d["Y"])
+    S = oracle.rates(blob, d["P"], d["T"], d["Y"], mech.nr)["S"]
+    for ref in ("wdot_scalar", "wdot_vec"):
+        e = oracle.errors(w, d[ref], S)
+        assert e["norm_max"] <= TOL_FP64 and e["gross_max"] <= TOL_FP64, (ref, e)
+
+
+@pytest.mark.parametrize("factory", [synthetic.all_kinds, synthetic.h2o2_10sp, synthetic.gri_shape])
+@pytest.mark.parametrize("ng", [1, 31, 33, 1000])
+def test_fp64_matches_oracle_ragged_sizes(factory, ng):
+    mech = factory()
+    blob = pack.pack(mech).to_blob()
+    P, T, Y = synthetic.states(mech.ns, ng, seed=ng)
+    w = _run(GpuMechanism(blob), P, T, Y)
+    r = oracle.rates(blob, P, T, Y, mech.nr)
+    e = oracle.errors(w, r["wdot"], r["S"])
+    assert e["norm_max"] <= TOL_FP64 and e["gross_max"] <= TOL_FP64, e
+
+
+def test_fp64_exact_zeros_and_range_switch():
+    mech = synthetic.all_kinds()
+    blob = pack.pack(mech).to_blob()
+    ng = 257
+    P, T, Y = synthetic.states(mech.ns, ng, seed=5)
+    Y[:, ::3] = 0.0
+    Y[0, ::3] = 1.0                      # pure species
+    Y[::2, 1::3] = 0.0
+    Y /= Y.sum(axis=0, keepdims=True)
+    T[::7] = 1000.0                       # every species switches range here
+    w = _run(GpuMechanism(blob), P, T, Y)
+    r = oracle.rates(blob, P, T, Y, mech.nr)
+    e = oracle.errors(w, r["wdot"], r["S"])
+    assert np.all(np.isfinite(w))
+    assert e["norm_max"] <= TOL_FP64 and e["gross_max"] <= TOL_FP64, e
+
+
+def test_fp64_empty_input_is_a_no_op():
+    import torch
+    gm = GpuMechanism(synthetic.h2o2_10sp())
+    z = torch.empty(0, dtype=torch.float64, device="cuda")
+    w = gm.getrates(z, z, torch.empty(gm.ns, 0, dtype=torch.float64, device="cuda"))
+    assert w.shape == (gm.ns, 0)
+
+
+def test_fp64_full_size_53_325_subsample_and_mass():
+    """2^20 points of the 53/325 workload; the oracle checks a seeded subsample."""
+    mech = synthetic.gri_shape()
+    blob = pack.pack(mech).to_blob()
+    ng = 1 << 20
+    P, T, Y = synthetic.states(mech.ns, ng, seed=11)
+    w = _run(GpuMechanism(blob), P, T, Y)
+    assert np.all(np.isfinite(w))
+    idx = np.sort(np.random.default_rng(0).choice(ng, 2048, replace=False))
+    r = oracle.rates(blob, P[idx], T[idx], np.ascontiguousarray(Y[:, idx]), mech.nr)
+    e = oracle.errors(w[:, idx], r["wdot"], r["S"])
+    assert e["norm_max"] <= TOL_FP64 and e["gross_max"] <= TOL_FP64, e
+
+
+def test_fp64_real_gri30_conserves_mass_at_size():
+    mech, d = load_golden("gri30")
+    blob = pack.pack(mech).to_blob()
+    ng = 1 << 18
+    P, T, Y = synthetic.states(mech.ns, ng, seed=3)
+    w = _run(GpuMechanism(blob), P, T, Y)
+    mw = np.array(mech.mw())[:, None]
+    idx = np.arange(0, ng, 97)
+    S = oracle.rates(blob, P[idx], T[idx], np.ascontiguousarray(Y[:, idx]), mech.nr)["S"]
+    resid = np.abs((mw * w[:, idx]).sum(axis=0))
+    assert np.all(resid <= 1e-12 * (mw * S).sum(axis=0))
+
+
+def test_host_pointer_path_matches_device_path():
+    mech = synthetic.gri_shape()
+    blob = pack.pack(mech).to_blob()
+    gm = GpuMechanism(blob)
+    ng = 300001
+    P, T, Y = synthetic.states(mech.ns, ng, seed=2)
+    w_dev = _run(gm, P, T, Y)
+    w_host = gm.getrates_host(P, T, Y)
+    assert np.array_equal(w_dev, w_host)
+
+
+def test_workspace_variant_large_mechanism():
+    mech, d = load_golden("jetsurf2")
+    blob = pack.pack(mech).to_blob()
+    gm = GpuMechanism(blob)
+    import torch
+    ng = d["T"].size
+    assert gm.workspace_bytes(ng) > 0        # 348 species: state in scratch
+    ws = torch.empty(gm.workspace_bytes(ng) // 8 + 64, dtype=torch.float64, device="cuda")
+    Pt, Tt, Yt = (torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (d["P"], d["T"], d["Y"]))
+    out = torch.empty_like(Yt)
+    gm.getrates_ws(Pt, Tt, Yt, out, ws)
+    torch.cuda.synchronize()
+    S = oracle.rates(blob, d["P"], d["T"], d["Y"], mech.nr)["S"]
+    e = oracle.errors(out.cpu().numpy(), d["wdot_scalar"], S)
+    assert e["norm_max"] <= TOL_FP64 and e["gross_max"] <= TOL_FP64, e
+
+
+def test_reference_wrapper_drop_in():
+    """getrates_hip_wrapper_v1 with the reference's signature and scratch."""
+    import ctypes
+    import torch
+    from chemgen_b200.runtime import lib
+    for name in ("gri30", "jetsurf2"):
+        mech, d = load_golden(name)
+        blob = pack.pack(mech).to_blob()
+        buf = ctypes.create_string_buffer(blob, len(blob))
+        assert lib().chemgen_init_constants(buf, len(blob)) == 0
+        ng = d["T"].size
+        Pt, Tt, Yt = (torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (d["P"], d["T"], d["Y"]))
+        w = torch.zeros_like(Yt)
+        eg = torch.empty_like(Yt)
+        c = torch.empty_like(Yt)
+        lib().getrates_hip_wrapper_v1(Pt.data_ptr(), Tt.data_ptr(), ng, Yt.data_ptr(), w.data_ptr(),
+                                      eg.data_ptr(), c.data_ptr())
+        assert lib().chemgen_last_wrapper_status() == 0
+        S = oracle.rates(blob, d["P"], d["T"], d["Y"], mech.nr)["S"]
+        e = oracle.errors(w.cpu().numpy(), d["wdot_scalar"], S)
+        assert e["norm_max"] <= TOL_FP64, e
+    assert lib().chemgen_free_constants() == 0
+    lib().getrates_hip_wrapper_v1(0, 0, 1, 0, 0, 0, 0)
+    assert lib().chemgen_last_wrapper_status() == 8
+
+
+def test_bad_arguments_return_status():
+    import torch
+    from chemgen_b200.runtime import ChemgenError
+    gm = GpuMechanism(synthetic.h2o2_10sp())
+    x = torch.ones(9, dtype=torch.float64, device="cuda")
+    with pytest.raises(ChemgenError):
+        gm.getrates_ptr(x.data_ptr() + 4, x.data_ptr(), 1, x.data_ptr(), x.data_ptr())
+    with pytest.raises(ChemgenError):
+        gm.getrates_ptr(x.data_ptr(), x.data_ptr(), -1, x.data_ptr(), x.data_ptr())
