@@ -43,6 +43,9 @@ def parse():
     ap.add_argument("--ng", type=int, default=1 << 20)
     ap.add_argument("--modes", default="fp64,mixed")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--clock-ms", type=float, default=1500.0, help="length of the clock-sampled timed pass")
+    ap.add_argument("--e2e-steps", type=int, default=-1, help="host-path steps (default min(steps, 50))")
+    ap.add_argument("--table", action="store_true", help="table-driven kernels instead of the generated ones")
     return ap.parse_args()
 
 
@@ -187,7 +190,7 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     mech = synthetic.gri_shape()
     blob = pack.pack(mech).to_blob()
-    gm = GpuMechanism(blob, device=local_rank)
+    gm = GpuMechanism(mech, device=local_rank, generated=not args.table)
     ng = args.ng
     P, T, Y = synthetic.states(mech.ns, ng, seed=1000 + rank)
     Pd, Td, Yd = (torch.from_numpy(x).to(dev) for x in (P, T, Y))
@@ -220,7 +223,7 @@ def run_ours(args, rank, world, local_rank):
             t = torch.tensor([ms], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
-        results[m] = {"ms_per_step": ms, "value": ng * world / (ms * 1e-3) / 1e6}
+        results[m] = {"ms_per_step": ms, "value": ng * world / (ms * 1e-3) / 1e6, "kernel": gm.kernel_kind(m)}
 
     # errors and CPU baseline on a bounded sample (rank 0, single GPU)
     err = {}
@@ -257,7 +260,7 @@ def run_ours(args, rank, world, local_rank):
     # clocks during a timed pass of the headline mode
     sampler = ClockSampler(local_rank)
     fn = lambda: gm.getrates(Pd, Td, Yd, out=W, mode=head, stream=stream)
-    steps_c = max(args.steps, int(math.ceil(1500.0 / max(results[head]["ms_per_step"], 1e-3))))
+    steps_c = max(args.steps, int(math.ceil(args.clock_ms / max(results[head]["ms_per_step"], 1e-3))))
     with sampler:
         ms_c = time_steps(fn, steps_c, 2, stream)
     clocks = sampler.summary()
@@ -268,13 +271,13 @@ def run_ours(args, rank, world, local_rank):
     Wh = torch.empty_like(Yh).pin_memory()
     for _ in range(2):
         gm.getrates_host(Ph, Th, Yh, out=Wh.numpy(), mode=head)
-    k_e2e = max(3, min(args.steps, 50))
+    k_e2e = max(1, min(args.steps, 50)) if args.e2e_steps < 0 else args.e2e_steps
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(k_e2e):
         gm.getrates_host(Ph, Th, Yh, out=Wh.numpy(), mode=head)
-    e2e_s = (time.perf_counter() - t0) / k_e2e
+    e2e_s = (time.perf_counter() - t0) / max(k_e2e, 1)
     if world > 1:
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

@@ -53,7 +53,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if ptxas_info or verbose:
             sys.stderr.write(r.stderr)
     if force or not os.path.exists(OUT) or any(os.path.getmtime(o) > os.path.getmtime(OUT) for o in objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", OUT] + objs + ["-Xlinker", "-soname=libchemgen_b200.so",
+                                                                "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -31,6 +31,12 @@ size_t mixed_workspace_bytes(const MixedPlan* p, int64_t ng);
 
 struct chemgen_handle {
     int device = 0;
+    uint64_t fingerprint = 0;
+    // kernels generated for this exact mechanism (generate_chemistry.py --language cuda)
+    chemgen_kernel_fn gen_fn = nullptr;
+    unsigned gen_modes = 0;
+    int use_generated = 1;
+    int gen_version = -1;
     int ns = 0, nr = 0;
     cg::DevMech m{};
     void* dbuf = nullptr;
@@ -70,6 +76,45 @@ int status_of(cudaError_t e) {
 }
 
 bool aligned8(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 7u) == 0; }
+
+// Registry of generated kernel modules, keyed by blob fingerprint.
+struct Registered {
+    uint64_t fp;
+    int ns, nr;
+    unsigned modes;
+    chemgen_kernel_fn fn;
+};
+std::mutex& reg_mu() {
+    static std::mutex m;
+    return m;
+}
+std::vector<Registered>& registry() {
+    static std::vector<Registered> r;
+    return r;
+}
+int g_reg_version = 0;
+
+uint64_t fnv1a(const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    uint64_t h = 0xcbf29ce484222325ull;
+    for (size_t i = 0; i < n; ++i) {
+        h ^= b[i];
+        h *= 0x100000001b3ull;
+    }
+    return h;
+}
+
+void refresh_generated(chemgen_handle* h) {
+    std::lock_guard<std::mutex> lk(reg_mu());
+    if (h->gen_version == g_reg_version) return;
+    h->gen_version = g_reg_version;
+    for (const Registered& r : registry())
+        if (r.fp == h->fingerprint && r.ns == h->ns && r.nr == h->nr) {
+            h->gen_fn = r.fn;
+            h->gen_modes = r.modes;
+        }
+}
+
 
 // Host image of the device tables; offsets are relative to the buffer start.
 struct Builder {
@@ -289,6 +334,7 @@ size_t fp64_ws_bytes(const chemgen_handle* h, int64_t ng) {
 }
 
 size_t ws_bytes_for(const chemgen_handle* h, int mode, int64_t ng) {
+    if (h->use_generated && h->gen_fn && (mode == 0 || mode == 1) && (h->gen_modes & (1u << mode))) return 0;
     if (mode == CHEMGEN_MODE_FP64) return fp64_ws_bytes(h, ng);
     if (mode == CHEMGEN_MODE_MIXED && h->mixed) return cg::mixed_workspace_bytes(h->mixed, ng);
     return 0;
@@ -308,6 +354,10 @@ int check_args(const chemgen_handle* h, const double* P, const double* T, int64_
 // slices fit, at least one).
 int launch(chemgen_handle* h, int mode, const double* P, const double* T, int64_t ng, const double* Y, double* w,
            void* ws, size_t ws_bytes, cudaStream_t s) {
+    refresh_generated(h);
+    if (h->use_generated && h->gen_fn && (mode == CHEMGEN_MODE_FP64 || mode == CHEMGEN_MODE_MIXED) &&
+        (h->gen_modes & (1u << mode)))
+        return h->gen_fn(mode, P, T, ng, Y, w, s);
     if (mode == CHEMGEN_MODE_FP64) {
         int64_t slices = 0;
         if (!h->fp64_block) {
@@ -378,6 +428,7 @@ int chemgen_create(const void* blob, size_t nbytes, int device, chemgen_handle**
     chemgen_handle* h = new (std::nothrow) chemgen_handle();
     if (!h) return CHEMGEN_ERR_OUT_OF_MEMORY;
     h->device = device;
+    h->fingerprint = fnv1a(blob, nbytes);
     int st = build_tables(v, h);
     if (st) {
         delete h;
@@ -416,6 +467,28 @@ int chemgen_destroy(chemgen_handle* h) {
 }
 
 int chemgen_num_species(const chemgen_handle* h) { return h ? h->ns : -1; }
+
+int chemgen_register_kernels(uint64_t fingerprint, int ns, int nr, unsigned modes, chemgen_kernel_fn fn) {
+    if (!fn || ns <= 0 || nr < 0) return CHEMGEN_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lk(reg_mu());
+    registry().push_back(Registered{fingerprint, ns, nr, modes, fn});
+    ++g_reg_version;
+    return CHEMGEN_OK;
+}
+
+int chemgen_use_generated(chemgen_handle* h, int enable) {
+    if (!h) return CHEMGEN_ERR_INVALID_ARGUMENT;
+    h->use_generated = enable ? 1 : 0;
+    return CHEMGEN_OK;
+}
+
+int chemgen_kernel_kind(chemgen_handle* h, int mode) {
+    if (!h || (mode != CHEMGEN_MODE_FP64 && mode != CHEMGEN_MODE_MIXED)) return -1;
+    refresh_generated(h);
+    if (h->use_generated && h->gen_fn && (h->gen_modes & (1u << mode))) return 1;
+    if (mode == CHEMGEN_MODE_MIXED && !h->mixed) return -1;
+    return 0;
+}
 int chemgen_num_reactions(const chemgen_handle* h) { return h ? h->nr : -1; }
 
 int chemgen_getrates_ex(chemgen_handle* h, int mode, const double* P, const double* T, int64_t ng, const double* Y,

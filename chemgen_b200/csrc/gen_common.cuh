@@ -1,0 +1,81 @@
+// Helpers shared by the mechanism-specialised kernels that
+// chemgen_b200/emit_cuda.py writes (generate_chemistry.py --language cuda).
+//
+// A generated kernel handles one grid point per thread.  Species indices,
+// stoichiometry and coefficients are compile-time constants; the wdot
+// accumulators are registers; C and EGp = exp(smh) * Patm/(R0 T) (FP64) or the
+// log2 Gibbs terms (mixed) live in shared memory as [species][thread].
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/chemgen_b200.h"
+
+namespace cgg {
+
+constexpr double kR0 = 8.314510e+07;
+constexpr double kPatm = 1013250.0;
+constexpr double kLog2e = 1.4426950408889634074;
+constexpr double kLn10 = 2.302585092994045684;
+
+// Newton-refined reciprocal (two iterations from the hardware estimate).
+__device__ __forceinline__ double rcp(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+
+// ---------------------------------------------------------------- mixed
+// 2^a for an FP64 exponent a, returned as FP64 with about 2^-22 relative
+// error: a = n + f with n = nearest integer (round-to-nearest by adding
+// 1.5*2^52), 2^f from the SFU's ex2 on FP32, and 2^n folded into the FP64
+// exponent field with integer arithmetic.  `scale` multiplies 2^f (an FP32
+// product, e.g. of concentrations) and `eoff` is an extra integer exponent.
+// Results below 2^-1022 flush to zero; above 2^1023 they become +inf.
+__device__ __forceinline__ float ex2f(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float lg2f(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Split a (|a| < 2^30) into integer n and fraction f in [-0.5, 0.5].
+__device__ __forceinline__ void split2(double a, int& n, float& f) {
+    const double magic = 6755399441055744.0;   // 1.5 * 2^52
+    const double t = a + magic;
+    n = __double2loint(t);
+    f = (float)(a - (t - magic));
+}
+
+// FP32 value v (>= 0 or < 0) times 2^k as FP64, by integer exponent arithmetic.
+__device__ __forceinline__ double f32_scaled_to_f64(float v, int k) {
+    const unsigned int b = __float_as_uint(v);
+    const unsigned int ef = (b >> 23) & 0xffu;
+    if (ef == 0u) return 0.0;                         // zero (FP32 subnormals flushed)
+    int e = (int)ef - 127 + k + 1023;
+    e = max(0, min(e, 2047));
+    const unsigned int hi = (b & 0x80000000u) | ((unsigned int)e << 20) | ((b & 0x7fffffu) >> 3);
+    const unsigned int lo = (b & 0x7u) << 29;
+    const double r = __hiloint2double((int)hi, (int)lo);
+    return e == 0 ? 0.0 : (e == 2047 ? __longlong_as_double(0x7ff0000000000000LL | ((long long)(b & 0x80000000u) << 32)) : r);
+}
+
+// q = 2^a * prod  (prod an FP32 product of scaled concentrations, eoff the
+// integer exponent that undoes their scaling).
+__device__ __forceinline__ double rate2(double a, float prod, int eoff) {
+    int n;
+    float f;
+    split2(a, n, f);
+    return f32_scaled_to_f64(ex2f(f) * prod, n + eoff);
+}
+
+}  // namespace cgg
+

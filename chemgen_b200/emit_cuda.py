@@ -1,0 +1,500 @@
+"""``--language cuda``: emit mechanism-specialised sm_100a getrates kernels.
+
+The reference renders one Jinja template per reaction into straight-line
+Python/Fortran/HIP (``chemgen/chemistry.py:269-321``).  This emitter does the
+same for CUDA: every reaction becomes a few lines with its coefficients and
+species slots as compile-time constants, so the kernel carries no table
+lookups or index arithmetic, and the per-species wdot accumulators are
+registers.  Two kernels are written per mechanism:
+
+* ``fp64``  -- the reference's arithmetic in FP64 (reactions/*.j2);
+* ``mixed`` -- exponents (Arrhenius, Gibbs differences -> Kc) and the wdot
+  sums in FP64, 2^f / concentration products / falloff blending in FP32.
+
+The module registers itself with libchemgen_b200.so at load time under the
+64-bit FNV-1a fingerprint of the mechanism's packed blob, after which
+``chemgen_create`` on the same blob dispatches to it.
+"""
+from __future__ import annotations
+
+import hashlib
+import math
+import os
+import subprocess
+from typing import Dict, List, Optional, Tuple
+
+from .mechanism import RC_CAL, Mechanism, Reaction
+from .pack import pack, r15, smh_coefs
+
+LOG2E = 1.4426950408889634074
+LN10 = 2.302585092994045684
+LOG10_2 = 0.30102999566398119521
+CSCALE_LOG2 = 32          # mixed: concentrations are stored as C * 2^32 in FP32
+# register-resident wdot accumulators up to this many species
+MAX_REG_SPECIES = 72
+
+
+def fingerprint(blob: bytes) -> int:
+    """64-bit FNV-1a of the packed blob (same function as capi.cu)."""
+    h = 0xcbf29ce484222325
+    for b in blob:
+        h ^= b
+        h = (h * 0x100000001b3) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def _d(x: float) -> str:
+    """A double literal that round-trips."""
+    if x == 0.0:
+        return "0.0"
+    if math.isinf(x):
+        return "(1.0/0.0)" if x > 0 else "(-1.0/0.0)"
+    return repr(float(x))
+
+
+def _f(x: float) -> str:
+    return repr(float(x)) + "f"
+
+
+class _Emitter:
+    def __init__(self, mech: Mechanism, block: int):
+        self.mech = mech
+        self.ns = mech.ns
+        self.idx = mech.species_index()
+        self.block = block
+        self.reg_w = self.ns <= MAX_REG_SPECIES
+        self.has_m = any(r.uses_m for r in mech.reactions)
+
+    # ------------------------------------------------------------- helpers
+    def C(self, sp: str) -> str:
+        return f"sC[{self.idx[sp]}][t]"
+
+    def E(self, sp: str) -> str:
+        return f"sE[{self.idx[sp]}][t]"
+
+    def W(self, sp: str) -> str:
+        k = self.idx[sp]
+        return f"w{k}" if self.reg_w else f"sW[{k}][t]"
+
+    @staticmethod
+    def _pow(x: str, nu: float) -> str:
+        if nu == 1.0:
+            return x
+        if nu == 2.0:
+            return f"({x}*{x})"
+        if nu == 3.0:
+            return f"({x}*{x}*{x})"
+        return f"pow({x}, {_d(nu)})"
+
+    def prod(self, side: Dict[str, float], fn) -> str:
+        terms = [self._pow(fn(sp), nu) for sp, nu in side.items()]
+        return "*".join(terms) if terms else "1.0"
+
+    def scatter(self, r: Reaction, rr: str) -> List[str]:
+        out = []
+        for sp, nu in r.reactants.items():
+            w = self.W(sp)
+            out.append(f"{w} = fma({_d(-nu)}, {rr}, {w});" if nu != 1.0 else f"{w} -= {rr};")
+        for sp, nu in r.products.items():
+            w = self.W(sp)
+            out.append(f"{w} = fma({_d(nu)}, {rr}, {w});" if nu != 1.0 else f"{w} += {rr};")
+        return out
+
+    @staticmethod
+    def arr64(A: float, b: float, Ea: float) -> str:
+        """A T^b exp(-Ea/(Rc T)) as one FP64 exp (reactions/standard.j2:4)."""
+        A, Ea = r15(A), r15(Ea)
+        if A == 0.0:
+            return "0.0"
+        lnA = math.log(abs(A))
+        th = Ea / RC_CAL
+        sgn = "-" if A < 0 else ""
+        parts = [_d(lnA)]
+        if b != 0.0:
+            parts = [f"fma({_d(b)}, lnT, {_d(lnA)})"]
+        if th != 0.0:
+            parts.append(f"- {_d(th)}*invT")
+        if b == 0.0 and th == 0.0:
+            return _d(A)
+        return f"{sgn}exp({' '.join(parts)})"
+
+    @staticmethod
+    def arr2(A: float, b: float, Ea: float) -> Tuple[str, bool]:
+        """log2 of |A T^b exp(-Ea/(Rc T))| as an FP64 expression, and the sign."""
+        A, Ea = r15(A), r15(Ea)
+        l2A = math.log2(abs(A)) if A != 0.0 else -2000.0
+        th2 = Ea / RC_CAL * LOG2E
+        e = _d(l2A)
+        if b != 0.0:
+            e = f"fma({_d(b)}, lnT2, {_d(l2A)})"    # b * log2 T
+        if th2 != 0.0:
+            e = f"fma({_d(-th2)}, invT, {e})"
+        return e, A < 0
+
+    # --------------------------------------------------------------- fp64
+    def falloff64(self, r: Reaction) -> List[str]:
+        L = []
+        L.append(f"const double kinf = {self.arr64(*r.arh)};")
+        L.append(f"const double k0 = {self.arr64(*r.low)};")
+        L.append("const double Pr = k0 * M * rcp(kinf);")
+        if r.kind == "troe":
+            a, T3, T1 = (r15(x) for x in r.troe[:3])
+            fc = f"fma({_d(r15(1.0 - a))}, exp({_d(-1.0 / T3)}*Tv), {_d(a)}*exp({_d(-1.0 / T1)}*Tv))"
+            if len(r.troe) == 4 and r.troe[3] != 0.0:
+                fc = f"({fc} + exp({_d(-r15(r.troe[3]))}*invT))"
+            L.append(f"const double Fc = {fc};")
+            L.append("const double lFc = log10(Fc);")
+            L.append("const double lp = log10(Pr) + fma(-0.67, lFc, -0.4);")
+            L.append("const double f1 = lp * rcp(fma(-0.14, lp, fma(-1.27, lFc, 0.75)));")
+            L.append(f"const double F = exp({_d(LN10)} * lFc * rcp(fma(f1, f1, 1.0)));")
+        elif r.kind == "sri":
+            s = list(r.sri) + ([1.0, 0.0] if len(r.sri) == 3 else [])
+            L.append("const double lp = log10(Pr);")
+            L.append("const double X = rcp(fma(lp, lp, 1.0));")
+            L.append(f"const double base = fma({_d(s[0])}, exp({_d(-s[1])}*invT), exp({_d(-1.0 / s[2])}*Tv));")
+            L.append(f"const double F = {_d(s[3])} * exp(fma(X, log(base), {_d(s[4])}*lnT));")
+        else:
+            L.append("const double F = 1.0;")
+        L.append("const double kf = kinf * (Pr * rcp(1.0 + Pr)) * F;")
+        return L
+
+    def plog64(self, r: Reaction) -> List[str]:
+        levels: Dict[float, List] = {}
+        for (p, A, b, Ea) in r.plog:
+            levels.setdefault(r15(p), []).append((A, b, Ea))
+        ps = sorted(levels)
+
+        def ksum(p):
+            return " + ".join(f"({self.arr64(A, b, Ea)})" for (A, b, Ea) in levels[p])
+
+        L = ["double kf;"]
+        L.append(f"if (Pv < {_d(ps[0])}) {{ kf = {ksum(ps[0])}; }}")
+        for lo, hi in zip(ps[:-1], ps[1:]):
+            llo, lhi = r15(math.log(lo)), r15(math.log(hi))
+            L.append(f"else if (Pv < {_d(hi)}) {{ const double kl = log({ksum(lo)}); const double kh = log({ksum(hi)}); "
+                     f"kf = exp(kl + (kh - kl) * (lnP - {_d(llo)}) * {_d(1.0 / (lhi - llo))}); }}")
+        L.append(f"else {{ kf = {ksum(ps[-1])}; }}")
+        return L
+
+    def reaction64(self, r: Reaction) -> List[str]:
+        L = [f"{{ // {r.equation}"]
+        body = []
+        if r.uses_m:
+            m = "ctot"
+            for sp, e in r.efficiencies.items():
+                m = f"fma({_d(r15(e))}, {self.C(sp)}, {m})"
+            body.append(f"const double M = {m};")
+        if r.kind in ("standard", "third_body"):
+            body.append(f"const double kf = {self.arr64(*r.arh)};")
+        elif r.kind == "plog":
+            body += self.plog64(r)
+        else:
+            body += self.falloff64(r)
+        qf = f"kf*{self.prod(r.reactants, self.C)}"
+        if r.reversible:
+            num = self.prod(r.reactants, self.E)
+            den = self.prod(r.products, self.E)
+            body.append(f"const double rr = {qf} - kf*({num})*rcp({den})*{self.prod(r.products, self.C)};")
+        else:
+            body.append(f"const double rr = {qf};")
+        rr = "(M*rr)" if r.kind == "third_body" else "rr"
+        body += self.scatter(r, rr)
+        L += ["  " + x for x in body] + ["}"]
+        return L
+
+    # -------------------------------------------------------------- mixed
+    def cprod32(self, side: Dict[str, float]) -> Tuple[str, int]:
+        """FP32 product of scaled concentrations and its total order."""
+        terms, order = [], 0
+        for sp, nu in side.items():
+            x = f"sc[{self.idx[sp]}][t]"
+            if nu in (1.0, 2.0, 3.0):
+                terms += [x] * int(nu)
+                order += int(nu)
+            else:
+                return "", -1
+        return ("*".join(terms) if terms else "1.0f"), order
+
+    def gsum(self, r: Reaction) -> str:
+        """sum nu_r G_r - sum nu_p G_p with G = log2(EGp) (FP64, shared memory)."""
+        terms = [(nu, sp) for sp, nu in r.reactants.items()] + [(-nu, sp) for sp, nu in r.products.items()]
+        expr = None
+        for coef, sp in terms:
+            g = f"sG[{self.idx[sp]}][t]"
+            if expr is None:
+                expr = g if coef == 1.0 else f"{_d(coef)}*{g}"
+            elif coef == 1.0:
+                expr = f"({expr} + {g})"
+            elif coef == -1.0:
+                expr = f"({expr} - {g})"
+            else:
+                expr = f"fma({_d(coef)}, {g}, {expr})"
+        return expr
+
+    def falloff32(self, r: Reaction) -> List[str]:
+        """log2 kf of a falloff reaction: FP64 exponents, FP32 blending."""
+        L = []
+        ainf, _ = self.arr2(*r.arh)
+        a0, _ = self.arr2(*r.low)
+        L.append(f"const double ainf = {ainf};")
+        # Pr = 2^(a0 - ainf) * M ; M is carried as Ms = M * 2^32 in FP32
+        L.append(f"int npr; float fpr; cgg::split2({a0} - ainf, npr, fpr);")
+        L.append("float mpr = cgg::ex2f(fpr) * Ms;")
+        L.append("int ex = ((__float_as_int(mpr) >> 23) & 0xff) - 126; npr += ex - 32;")
+        L.append("mpr = __int_as_float((__float_as_int(mpr) & 0x807fffff) | (126 << 23));   // [0.5, 1)")
+        # lg2 Pr/(1+Pr) = npr + lg2(mpr) - lg2(1+Pr) (Pr < 1) or -lg2(1+1/Pr)
+        L.append("float l2r; int nfix = 0; const float l2pr = (float)npr + cgg::lg2f(mpr);")
+        L.append("if (npr < 0) { const float pr = npr > -126 ? ldexpf(mpr, npr) : 0.0f; "
+                 "l2r = cgg::lg2f(mpr) - cgg::lg2f(1.0f + pr); nfix = npr; }")
+        L.append("else { const float ipr = npr < 126 ? ldexpf(1.0f / mpr, -npr) : 0.0f; l2r = -cgg::lg2f(1.0f + ipr); }")
+        if r.kind == "troe":
+            a, T3, T1 = (r15(x) for x in r.troe[:3])
+            fc = (f"fmaf({_f(r15(1.0 - a))}, cgg::ex2f({_f(-LOG2E / T3)}*Tf), "
+                  f"{_f(a)}*cgg::ex2f({_f(-LOG2E / T1)}*Tf))")
+            if len(r.troe) == 4 and r.troe[3] != 0.0:
+                fc = f"({fc} + cgg::ex2f({_f(-LOG2E * r15(r.troe[3]))}*invTf))"
+            L.append(f"const float Fc = {fc};")
+            L.append(f"const float lFc = {_f(LOG10_2)} * cgg::lg2f(Fc);")
+            L.append(f"const float lp = {_f(LOG10_2)} * l2pr + fmaf(-0.67f, lFc, -0.4f);")
+            L.append("const float f1 = __fdividef(lp, fmaf(-0.14f, lp, fmaf(-1.27f, lFc, 0.75f)));")
+            L.append(f"const float l2F = {_f(1.0 / LOG10_2)} * __fdividef(lFc, fmaf(f1, f1, 1.0f));")
+        elif r.kind == "sri":
+            s = list(r.sri) + ([1.0, 0.0] if len(r.sri) == 3 else [])
+            L.append(f"const float lp = {_f(LOG10_2)} * l2pr;")
+            L.append("const float X = __fdividef(1.0f, fmaf(lp, lp, 1.0f));")
+            L.append(f"const float base = fmaf({_f(s[0])}, cgg::ex2f({_f(-LOG2E * s[1])}*invTf), "
+                     f"cgg::ex2f({_f(-LOG2E / s[2])}*Tf));")
+            L.append(f"const float l2F = {_f(math.log2(s[3]) if s[3] > 0 else -200.0)} + X*cgg::lg2f(base) "
+                     f"+ {_f(s[4])}*lnT2f;")
+        else:
+            L.append("const float l2F = 0.0f;")
+        L.append("const double akf = ainf + ((double)nfix + (double)(l2r + l2F));")
+        return L
+
+    def reaction32(self, r: Reaction) -> List[str]:
+        L = [f"{{ // {r.equation}"]
+        body = []
+        cf, of = self.cprod32(r.reactants)
+        cb, ob = self.cprod32(r.products)
+        if of < 0 or ob < 0 or r.kind == "plog":
+            # fractional stoichiometry or PLOG: the FP64 formula of this reaction
+            return self.reaction32_fallback(r)
+        if r.uses_m:
+            m = "ctot32"
+            for sp, e in r.efficiencies.items():
+                m = f"fmaf({_f(r15(e))}, sc[{self.idx[sp]}][t], {m})"
+            body.append(f"const float Ms = {m};")
+        if r.kind in ("standard", "third_body"):
+            a, neg = self.arr2(*r.arh)
+            body.append(f"const double akf = {a};")
+            if r.kind == "third_body":
+                cf, of = f"{cf}*Ms", of + 1
+                cb, ob = f"{cb}*Ms", ob + 1
+            sgn = "-" if neg else ""
+        else:
+            body += self.falloff32(r)
+            sgn = ""
+        body.append(f"double rr = {sgn}cgg::rate2(akf, {cf}, {-CSCALE_LOG2 * of});")
+        if r.reversible:
+            body.append(f"rr -= {sgn}cgg::rate2(akf + {self.gsum(r)}, {cb}, {-CSCALE_LOG2 * ob});")
+        body += self.scatter(r, "rr")
+        L += ["  " + x for x in body] + ["}"]
+        return L
+
+    def reaction32_fallback(self, r: Reaction) -> List[str]:
+        """FP64 evaluation inside the mixed kernel (fractional nu, PLOG)."""
+        L = [f"{{ // {r.equation} (FP64)"]
+        body = []
+        C = lambda sp: f"((double)sc[{self.idx[sp]}][t] * {_d(2.0 ** -CSCALE_LOG2)})"
+        E = lambda sp: f"exp2(sG[{self.idx[sp]}][t])"
+        if r.uses_m:
+            m = "((double)ctot32 * " + _d(2.0 ** -CSCALE_LOG2) + ")"
+            for sp, e in r.efficiencies.items():
+                m = f"fma({_d(r15(e))}, {C(sp)}, {m})"
+            body.append(f"const double M = {m};")
+        if r.kind in ("standard", "third_body"):
+            body.append(f"const double kf = {self.arr64(*r.arh)};")
+        elif r.kind == "plog":
+            body += self.plog64(r)
+        else:
+            body += self.falloff64(r)
+        qf = f"kf*{self.prod(r.reactants, C)}"
+        if r.reversible:
+            body.append(f"const double rr = {qf} - kf*({self.prod(r.reactants, E)})*rcp({self.prod(r.products, E)})"
+                        f"*{self.prod(r.products, C)};")
+        else:
+            body.append(f"const double rr = {qf};")
+        rr = "(M*rr)" if r.kind == "third_body" else "rr"
+        body += self.scatter(r, rr)
+        L += ["  " + x for x in body] + ["}"]
+        return L
+
+    # ------------------------------------------------------------- kernels
+    def prologue(self, mixed: bool) -> List[str]:
+        """Load P, T, Y; C = Y/W * P/(R0 sum(Y/W) T) (ytoc.j2); Gibbs (exp_g.j2)."""
+        ns, B = self.ns, self.block
+        L = []
+        L.append("const int t = threadIdx.x;")
+        L.append(f"const int64_t i = (int64_t)blockIdx.x * {B} + t;")
+        L.append("const bool act = i < ng;")
+        L.append("const double Tv = act ? T[i] : 1000.0;")
+        L.append(f"const double Pv = act ? P[i] : {_d(1013250.0)};")
+        L.append("const double lnT = log(Tv), invT = rcp(Tv);")
+        if any(r.kind == "plog" for r in self.mech.reactions):
+            L.append("const double lnP = log(Pv);")
+        mw = self.mech.mw()
+        tmp = "sC" if not mixed else "sG"          # unscaled Y/W, overwritten below
+        L.append("double csum = 0.0;")
+        for k in range(ns):
+            L.append(f"{{ const double c = (act ? Y[(int64_t){k} * ng + i] : 1.0) * {_d(1.0 / r15(mw[k]))}; "
+                     f"{tmp}[{k}][t] = c; csum += c; }}")
+        L.append(f"const double fac = Pv * rcp({_d(8.314510e+07)} * csum * Tv);")
+        L.append("double ctot = 0.0;")
+        if not mixed:
+            for k in range(ns):
+                L.append(f"{{ const double c = sC[{k}][t] * fac; sC[{k}][t] = c; ctot += c; }}")
+            L.append(f"const double pfac = {_d(1013250.0 / 8.314510e+07)} * invT;")
+        else:
+            L.append(f"const double facs = fac * {_d(2.0 ** CSCALE_LOG2)};")
+            for k in range(ns):
+                L.append(f"{{ const double c = sG[{k}][t] * facs; sc[{k}][t] = (float)c; ctot += c; }}")
+            L.append("const float ctot32 = (float)ctot;")
+            L.append(f"const double lnT2 = lnT * {_d(LOG2E)};")
+            L.append(f"const double lpfac2 = {_d(math.log2(1013250.0 / 8.314510e+07))} - lnT2;")
+            L.append("const float Tf = (float)Tv, invTf = (float)invT, lnT2f = (float)lnT2;")
+        for k, sp in enumerate(self.mech.species):
+            lo, hi = smh_coefs(sp.nasa_low), smh_coefs(sp.nasa_high)
+            if lo == hi:
+                sel, pre = [_d(x) for x in lo], ""
+            else:
+                pre = f"const bool lo{k} = Tv < {_d(sp.t_ranges[1])}; "
+                sel = [f"(lo{k} ? {_d(a)} : {_d(b)})" for a, b in zip(lo, hi)]
+            poly = (f"fma(fma(fma(fma({sel[5]}, Tv, {sel[4]}), Tv, {sel[3]}), Tv, {sel[2]}), Tv, "
+                    f"fma({sel[1]}, lnT, {sel[0]})) - {sel[6]} * invT")
+            if not mixed:
+                L.append(f"{{ {pre}sE[{k}][t] = exp({poly}) * pfac; }}")
+            else:
+                L.append(f"{{ {pre}sG[{k}][t] = fma({poly}, {_d(LOG2E)}, lpfac2); }}")
+        if self.reg_w:
+            L.append("double " + ", ".join(f"w{k} = 0.0" for k in range(ns)) + ";")
+        else:
+            for k in range(ns):
+                L.append(f"sW[{k}][t] = 0.0;")
+        return L
+
+    def epilogue(self) -> List[str]:
+        L = ["if (act) {"]
+        for k in range(self.ns):
+            w = f"w{k}" if self.reg_w else f"sW[{k}][t]"
+            L.append(f"  wdot[(int64_t){k} * ng + i] = {w};")
+        L.append("}")
+        return L
+
+    def smem_bytes(self, mixed: bool) -> int:
+        per = (16 if not mixed else 12) + (0 if self.reg_w else 8)
+        return per * self.ns * self.block
+
+    def kernel(self, mixed: bool) -> str:
+        ns, B = self.ns, self.block
+        name = "cg_gen_mixed" if mixed else "cg_gen_fp64"
+        L = [f"__global__ void __launch_bounds__({B}) {name}(const double* __restrict__ P, "
+             "const double* __restrict__ T, const double* __restrict__ Y, double* __restrict__ wdot, int64_t ng) {"]
+        # dynamic shared memory: [array][species][thread]
+        L.append("  extern __shared__ __align__(16) unsigned char dsm[];")
+        if not mixed:
+            L.append(f"  double (*sC)[{B}] = reinterpret_cast<double (*)[{B}]>(dsm);")
+            L.append(f"  double (*sE)[{B}] = reinterpret_cast<double (*)[{B}]>(dsm + {ns * B * 8});")
+            off = 2 * ns * B * 8
+        else:
+            L.append(f"  double (*sG)[{B}] = reinterpret_cast<double (*)[{B}]>(dsm);")
+            L.append(f"  float (*sc)[{B}] = reinterpret_cast<float (*)[{B}]>(dsm + {ns * B * 8});")
+            off = ns * B * 12
+        if not self.reg_w:
+            L.append(f"  double (*sW)[{B}] = reinterpret_cast<double (*)[{B}]>(dsm + {off});")
+        L += ["  " + x for x in self.prologue(mixed)]
+        for r in self.mech.reactions:
+            L += ["  " + x for x in (self.reaction32(r) if mixed else self.reaction64(r))]
+        L += ["  " + x for x in self.epilogue()]
+        L.append("}")
+        return "\n".join(L)
+
+
+def choose_block(ns: int) -> int:
+    return 128 if ns <= 24 else 64
+
+
+def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = None) -> str:
+    blob = pack(mech).to_blob()
+    fp = fingerprint(blob)
+    block = block or choose_block(mech.ns)
+    em = _Emitter(mech, block)
+    ident = "".join(ch if ch.isalnum() else "_" for ch in (name or mech.name))
+    src = [
+        f"// Generated by chemgen_b200 (generate_chemistry.py --language cuda) for mechanism '{mech.name}':",
+        f"// {mech.ns} species, {mech.nr} reactions {mech.counts()}.",
+        f"// Blob fingerprint 0x{fp:016x}.  Target: sm_100a.",
+        '#include "gen_common.cuh"',
+        "using cgg::rcp;",
+        "namespace {",
+        em.kernel(False),
+        "",
+        em.kernel(True),
+        "",
+        "int launch(int mode, const double* P, const double* T, int64_t ng, const double* Y, double* wdot, void* s) {",
+        "  if (ng <= 0) return CHEMGEN_OK;",
+        "  static bool attrs = false;",
+        "  if (!attrs) {",
+        f"    if (cudaFuncSetAttribute(cg_gen_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, {em.smem_bytes(False)}) != cudaSuccess ||",
+        f"        cudaFuncSetAttribute(cg_gen_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, {em.smem_bytes(True)}) != cudaSuccess)",
+        "      return CHEMGEN_ERR_CUDA;",
+        "    attrs = true;",
+        "  }",
+        f"  const unsigned blocks = (unsigned)((ng + {block - 1}) / {block});",
+        "  cudaStream_t st = (cudaStream_t)s;",
+        f"  if (mode == CHEMGEN_MODE_FP64) cg_gen_fp64<<<blocks, {block}, {em.smem_bytes(False)}, st>>>(P, T, Y, wdot, ng);",
+        f"  else if (mode == CHEMGEN_MODE_MIXED) cg_gen_mixed<<<blocks, {block}, {em.smem_bytes(True)}, st>>>(P, T, Y, wdot, ng);",
+        "  else return CHEMGEN_ERR_INVALID_ARGUMENT;",
+        "  return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA;",
+        "}",
+        "",
+        "struct Register {",
+        f"  Register() {{ chemgen_register_kernels(0x{fp:016x}ull, {mech.ns}, {mech.nr}, 3u, &launch); }}",
+        "} register_once;",
+        "}  // namespace",
+        "",
+        f'extern "C" unsigned long long chemgen_generated_fingerprint_{ident}(void) {{ return 0x{fp:016x}ull; }}',
+    ]
+    return "\n".join(src) + "\n"
+
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GEN_DIR = os.path.join(HERE, "_generated")
+
+
+def module_path(mech: Mechanism) -> str:
+    fp = fingerprint(pack(mech).to_blob())
+    return os.path.join(GEN_DIR, f"libcg_{fp:016x}.so")
+
+
+def build_module(mech: Mechanism, out: Optional[str] = None, verbose: bool = False, keep_source: bool = True) -> str:
+    """Emit and compile the mechanism's kernels into a shared library that
+    links libchemgen_b200.so and registers itself when loaded."""
+    from .build import ARCH, FLAGS, OUT as LIBMAIN, nvcc
+    os.makedirs(GEN_DIR, exist_ok=True)
+    so = out or module_path(mech)
+    src = so[:-3] + ".cu"
+    text = emit(mech)
+    with open(src, "w") as f:
+        f.write(text)
+    cmd = [nvcc()] + ARCH + FLAGS + ["-I", os.path.join(HERE, "csrc"), "-shared", "-o", so, src,
+                                     "-L", os.path.dirname(LIBMAIN), "-lchemgen_b200",
+                                     "-Xlinker", "-rpath=$ORIGIN/..", "-Xlinker", "-rpath=$ORIGIN",
+                                     "-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed on generated {src}:\n{r.stdout}\n{r.stderr[-4000:]}")
+    if verbose and r.stderr:
+        print(r.stderr)
+    return so

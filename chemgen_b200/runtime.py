@@ -40,7 +40,7 @@ def lib() -> ctypes.CDLL:
         return _lib
     if not os.path.exists(LIB_PATH):
         raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m chemgen_b200.build`")
-    L = ctypes.CDLL(LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
     vp, i64, sz, ci = ctypes.c_void_p, ctypes.c_int64, ctypes.c_size_t, ctypes.c_int
     L.chemgen_version.restype = ctypes.c_char_p
     L.chemgen_status_string.restype = ctypes.c_char_p
@@ -59,10 +59,14 @@ def lib() -> ctypes.CDLL:
     L.getrates_hip_wrapper_v1.argtypes = [vp, vp, ci, vp, vp, vp, vp]
     L.getrates_hip_wrapper_v1.restype = None
     L.chemgen_last_wrapper_status.argtypes = []
+    L.chemgen_use_generated.argtypes = [vp, ci]
+    L.chemgen_kernel_kind.argtypes = [vp, ci]
+    L.chemgen_register_kernels.argtypes = [ctypes.c_uint64, ci, ci, ctypes.c_uint, vp]
     for f in ("chemgen_create", "chemgen_destroy", "chemgen_num_species", "chemgen_num_reactions",
               "chemgen_getrates", "chemgen_getrates_ex", "chemgen_workspace_bytes", "chemgen_getrates_ws",
               "chemgen_getrates_host", "chemgen_init_constants", "chemgen_free_constants",
-              "chemgen_last_wrapper_status"):
+              "chemgen_last_wrapper_status", "chemgen_use_generated", "chemgen_kernel_kind",
+              "chemgen_register_kernels"):
         getattr(L, f).restype = ci
     _lib = L
     return L
@@ -92,13 +96,41 @@ def _stream(stream) -> int:
     return stream.cuda_stream
 
 
-class GpuMechanism:
-    """A mechanism loaded on one GPU (one chemgen_handle)."""
+_loaded_modules = {}
 
-    def __init__(self, mech: Union[Mechanism, bytes], device: int = 0):
+
+def load_generated(mech: Mechanism, build: bool = True) -> Optional[str]:
+    """Load (building first if needed) the kernels generated for `mech`
+    (generate_chemistry.py --language cuda); returns the module path or None."""
+    from . import emit_cuda
+    if mech.ns > emit_cuda.MAX_REG_SPECIES:
+        return None
+    path = emit_cuda.module_path(mech)
+    if path in _loaded_modules:
+        return path
+    if not os.path.exists(path):
+        if not build:
+            return None
+        emit_cuda.build_module(mech, out=path)
+    lib()
+    _loaded_modules[path] = ctypes.CDLL(path, mode=ctypes.RTLD_GLOBAL)
+    return path
+
+
+class GpuMechanism:
+    """A mechanism loaded on one GPU (one chemgen_handle).
+
+    generated=True loads the mechanism-specialised kernels (compiling them on
+    first use); generated=False keeps the table-driven kernels."""
+
+    def __init__(self, mech: Union[Mechanism, bytes], device: int = 0, generated: bool = False):
         self.blob = mech if isinstance(mech, (bytes, bytearray)) else pack(mech).to_blob()
         self.mech = None if isinstance(mech, (bytes, bytearray)) else mech
         self.device = device
+        if generated:
+            if self.mech is None:
+                raise ValueError("generated kernels need the Mechanism, not only its blob")
+            load_generated(self.mech)
         self._buf = ctypes.create_string_buffer(bytes(self.blob), len(self.blob))
         h = ctypes.c_void_p()
         check(lib().chemgen_create(self._buf, len(self.blob), device, ctypes.byref(h)), "chemgen_create")
@@ -120,6 +152,13 @@ class GpuMechanism:
     @property
     def handle(self) -> ctypes.c_void_p:
         return self._h
+
+    def kernel_kind(self, mode: str = "fp64") -> str:
+        k = lib().chemgen_kernel_kind(self._h, MODES[mode])
+        return {1: "generated", 0: "table", -1: "unavailable"}[k]
+
+    def use_generated(self, enable: bool) -> None:
+        check(lib().chemgen_use_generated(self._h, 1 if enable else 0), "chemgen_use_generated")
 
     def workspace_bytes(self, ng: int, mode: str = "fp64") -> int:
         out = ctypes.c_size_t()

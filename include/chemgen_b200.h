@@ -85,6 +85,20 @@ int chemgen_getrates_ws(chemgen_handle* h, int mode, const double* P, const doub
 int chemgen_getrates_host(chemgen_handle* h, int mode, const double* P, const double* T, int64_t ng,
                           const double* Y, double* wdot);
 
+/* Kernels generated for one mechanism (generate_chemistry.py --language cuda
+ * emits them; the reference's counterpart is its per-mechanism generated
+ * getrates, chemgen/chemistry.py:326-341).  A generated module calls
+ * chemgen_register_kernels when it is loaded; every handle whose blob has the
+ * same 64-bit FNV-1a fingerprint then runs the generated kernels instead of
+ * the table-driven ones.  chemgen_use_generated(h, 0) forces the
+ * table-driven kernels; chemgen_kernel_kind reports which kernel a mode
+ * runs: 1 generated, 0 table-driven, -1 unavailable. */
+typedef int (*chemgen_kernel_fn)(int mode, const double* P, const double* T, int64_t ng, const double* Y,
+                                 double* wdot, void* stream);
+int chemgen_register_kernels(uint64_t fingerprint, int ns, int nr, unsigned modes, chemgen_kernel_fn fn);
+int chemgen_use_generated(chemgen_handle* h, int enable);
+int chemgen_kernel_kind(chemgen_handle* h, int mode);
+
 /* Drop-in for the reference's process-global API.
  * chemgen_init_constants replaces copyConstantsToDevice
  * (chemgen/constants.py:119-240): it installs one process-wide mechanism.

@@ -15,6 +15,7 @@ def declared_functions():
     for h in ("chemgen_b200.h", "chemgen_b200_probe.h"):
         text = open(os.path.join(REPO, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        text = "\n".join(l for l in text.splitlines() if not l.lstrip().startswith("typedef"))
         for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\*?\s+\*?([a-z_][a-z0-9_]*)\s*\(", text,
                              flags=re.M):
             names.add(m.group(1))
