@@ -27,6 +27,11 @@ cudaError_t launch_getrates_mixed(const MixedPlan* p, const DevMech& m, const do
                                   const double* Y, double* wdot, int64_t ng, void* scratch, size_t scratch_bytes,
                                   cudaStream_t s);
 size_t mixed_workspace_bytes(const MixedPlan* p, int64_t ng);
+size_t deriv_workspace_bytes(int ns, int64_t ng);
+cudaError_t launch_jacobian(const DevMech& m, int precision, const double* P, const double* T, const double* Y,
+                            void* J, int64_t ng, double* scratch, int sm_count, cudaStream_t s);
+cudaError_t launch_vjp(const DevMech& m, const double* P, const double* T, const double* Y, const double* G, double* gT,
+                       double* gY, double* gP, int64_t ng, double* scratch, int sm_count, cudaStream_t s);
 }  // namespace cg
 
 struct chemgen_handle {
@@ -38,6 +43,7 @@ struct chemgen_handle {
     int use_generated = 1;
     int gen_version = -1;
     int ns = 0, nr = 0;
+    int max_side = 0;               // most species on one side of a reaction
     cg::DevMech m{};
     void* dbuf = nullptr;
     int sm_count = 0;
@@ -175,6 +181,7 @@ int build_tables(const cg_mech_view& v, chemgen_handle* h) {
         if (r >= fall0 && r < plog0) R.aux = r - fall0;
         else if (r >= plog0) R.aux = r - plog0;
         const int nre = rp[r + 1] - rp[r], npr = pp[r + 1] - pp[r];
+        h->max_side = std::max(h->max_side, std::max(nre, npr));
         bool compact = nre <= kMaxCompact && npr <= kMaxCompact;
         for (int j = rp[r]; compact && j < rp[r + 1]; ++j)
             compact = (rnu[j] == 1.0 || rnu[j] == 2.0 || rnu[j] == 3.0);
@@ -474,6 +481,35 @@ int chemgen_register_kernels(uint64_t fingerprint, int ns, int nr, unsigned mode
     registry().push_back(Registered{fingerprint, ns, nr, modes, fn});
     ++g_reg_version;
     return CHEMGEN_OK;
+}
+
+int chemgen_jacobian(chemgen_handle* h, int precision, const double* P, const double* T, int64_t ng,
+                     const double* Y, void* J, void* stream) {
+    int st = check_args(h, P, T, ng, Y, (const double*)J);
+    if (st || ng == 0) return st;
+    if (precision != 0 && precision != 1) return CHEMGEN_ERR_INVALID_ARGUMENT;
+    DeviceGuard g(h->device);
+    if (h->max_side > 16) return CHEMGEN_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lk(h->mu);
+    st = ensure_ws_locked(h, cg::deriv_workspace_bytes(h->ns, ng));
+    if (st) return st;
+    return status_of(cg::launch_jacobian(h->m, precision, P, T, Y, J, ng, (double*)h->ws, h->sm_count,
+                                         (cudaStream_t)stream));
+}
+
+int chemgen_getrates_vjp(chemgen_handle* h, const double* P, const double* T, int64_t ng, const double* Y,
+                         const double* G, double* gT, double* gY, double* gP, void* stream) {
+    int st = check_args(h, P, T, ng, Y, gY);
+    if (st || ng == 0) return st;
+    if (!G || !gT || !aligned8(G) || !aligned8(gT) || (gP && !aligned8(gP)))
+        return G && gT ? CHEMGEN_ERR_MISALIGNED : CHEMGEN_ERR_INVALID_ARGUMENT;
+    DeviceGuard g(h->device);
+    if (h->max_side > 16) return CHEMGEN_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lk(h->mu);
+    st = ensure_ws_locked(h, cg::deriv_workspace_bytes(h->ns, ng));
+    if (st) return st;
+    return status_of(cg::launch_vjp(h->m, P, T, Y, G, gT, gY, gP, ng, (double*)h->ws, h->sm_count,
+                                    (cudaStream_t)stream));
 }
 
 int chemgen_use_generated(chemgen_handle* h, int enable) {

@@ -1,0 +1,398 @@
+// Analytic derivatives of getrates: the dense Jacobian d wdot / d(T, Y) and
+// the adjoint (vector-Jacobian product), table-driven so that one compiled
+// kernel serves every mechanism.
+//
+// The reference has no derivative code (its torch prototype
+// chemgen/chemistry_nn.py:15-85 never ran); these kernels differentiate the
+// rate law of reactions/*.j2:
+//     wdot_k = sum_r nu_kr q_r,   q_r = m_r (qf_r - qb_r),   C = C(T, Y)
+// with
+//     dC_m/dY_j  = (ctot delta_mj - C_m) / (W_j S),  S = sum_j Y_j / W_j,
+//     dC_m/dT    = -C_m / T,   dM/dC_m = 1 + (eff_m - 1),
+//     d ln kf/dT = (b + theta/T) / T   (theta = Ea/Rc),
+//     d ln kb/dT = d ln kf/dT + sum nu_r dE_r - sum nu_p dE_p,
+//     dE_k       = d ln(exp(smh_k) Patm/(R0 T))/dT = d smh_k/dT - 1/T,
+//     falloff:   d ln kf = d ln kinf + g (d ln k0 - d ln kinf + d ln M) + d ln F|_Pr,
+//                g = 1/(1 + Pr) + d ln F / d ln Pr.
+// Mass-action derivatives use the product of the other factors, so species
+// at zero concentration keep exact derivatives.
+//
+// Layouts: J[(k*(ns+1) + c)*ng + i], column c = 0 for T and 1 + j for Y_j;
+// adjoint outputs gT[i], gY[j*ng + i], gP[i].  Per-point state (C, EGp, dE
+// and, for the Jacobian, the dense-M vector A) lives in a scratch buffer of
+// 4*ns*ng doubles laid out [array][species][point].
+#include <cuda_runtime.h>
+
+#include "cg_math.cuh"
+#include "rates_common.cuh"
+
+namespace cg {
+namespace {
+
+constexpr double kLn10 = 2.302585092994045684;
+
+struct DState {
+    double* C;
+    double* E;
+    double* D;
+    double* A;
+    int64_t s;       // stride between species (ng)
+};
+
+__device__ __forceinline__ double arr_ln(double lnA, double b, double theta, const PointT& pt) {
+    return fma(b, pt.lnT, lnA) - theta * pt.invT;
+}
+__device__ __forceinline__ double arr_dln(double b, double theta, const PointT& pt) {
+    return fma(theta, pt.invT, b) * pt.invT;
+}
+
+// Forward rate constant of a falloff reaction and its derivatives:
+// dlkf = d ln kf/dT at fixed M, gM = d ln kf/dM.
+__device__ void falloff_d(int kind, int flags, const DRxn& R, const DFall& f, double x2, double M, const PointT& pt,
+                          double& kf, double& dlkf, double& gM) {
+    const double lkinf = arr_ln(R.lnA, R.b, R.theta, pt);
+    const double lr = arr_ln(f.lnA0, f.b0, f.theta0, pt) - lkinf;
+    const double Pr = cgm::cg_exp_clamped(lr) * M * (f.sgn0 * R.sgn);
+    const double dlkinf = arr_dln(R.b, R.theta, pt);
+    const double dlPr = arr_dln(f.b0, f.theta0, pt) - dlkinf;
+    const double ipr = cgm::cg_rcp(1.0 + Pr);
+    double lnF = 0.0, gpr = ipr, dlF_T = 0.0;
+    if (kind == CG_TROE) {
+        const double e3 = cgm::cg_exp_clamped(-pt.T * f.p[1]);
+        const double e1 = cgm::cg_exp_clamped(-pt.T * f.p[3]);
+        double Fc = fma(f.p[0], e3, f.p[2] * e1);
+        double dFc = fma(-f.p[0] * f.p[1], e3, -f.p[2] * f.p[3] * e1);
+        if (flags & CG_F_TROE_T2) {
+            const double e2 = cgm::cg_exp_clamped(-x2 * pt.invT);
+            Fc += e2;
+            dFc = fma(x2 * pt.invT * pt.invT, e2, dFc);
+        }
+        const double lFc = cgm::cg_log10(Fc);
+        const double u = fma(lr, 1.0 / kLn10, cgm::cg_log10(M)) + fma(-0.67, lFc, -0.4);
+        const double nn = fma(-1.27, lFc, 0.75);
+        const double den = fma(-0.14, u, nn);
+        const double iden = cgm::cg_rcp(den);
+        const double f1 = u * iden;
+        const double q1 = cgm::cg_rcp(fma(f1, f1, 1.0));
+        lnF = kLn10 * lFc * q1;
+        const double dF_df1 = -2.0 * lFc * f1 * q1 * q1;
+        const double dF_dlpr = dF_df1 * nn * iden * iden;
+        const double df1_dlfc = (-0.67 * den + 1.1762 * u) * iden * iden;
+        const double dF_dlfc = fma(dF_df1, df1_dlfc, q1);
+        gpr = ipr + dF_dlpr;
+        dlF_T = dF_dlfc * dFc * cgm::cg_rcp(Fc);
+    } else if (kind == CG_SRI) {
+        const double lp = fma(lr, 1.0 / kLn10, cgm::cg_log10(M));
+        const double X = cgm::cg_rcp(fma(lp, lp, 1.0));
+        const double eb = cgm::cg_exp_clamped(-f.p[1] * pt.invT);
+        const double ec = cgm::cg_exp_clamped(-pt.T * f.p[2]);
+        const double base = fma(f.p[0], eb, ec);
+        const double dbase = fma(f.p[0] * f.p[1] * pt.invT * pt.invT, eb, -f.p[2] * ec);
+        const double lb = cgm::cg_log(base);
+        lnF = cgm::cg_log(f.p[3]) + fma(X, lb, x2 * pt.lnT);
+        gpr = ipr - 2.0 * lp * X * X * lb / kLn10;
+        dlF_T = fma(X, dbase * cgm::cg_rcp(base), x2 * pt.invT);
+    }
+    kf = R.sgn * cgm::cg_exp_clamped(lkinf + lnF) * (Pr * ipr);
+    dlkf = fma(gpr, dlPr, dlkinf) + dlF_T;
+    gM = gpr * cgm::cg_rcp(M);
+}
+
+// PLOG forward rate, d ln kf/dT and d ln kf/d ln P (plog.j2:4-38).
+__device__ void plog_d(const DevMech& m, int row, double P, double lnP, const PointT& pt, double& kf, double& dlkf,
+                       double& dlkf_lnP) {
+    const int l0 = __ldg(m.plog_ptr + row), l1 = __ldg(m.plog_ptr + row + 1);
+    int l = l0;
+    while (l < l1 && !(P < __ldg(m.plog_p + l))) ++l;
+    int la, lb;
+    if (l == l0) la = lb = l0;
+    else if (l == l1) la = lb = l1 - 1;
+    else {
+        la = l - 1;
+        lb = l;
+    }
+    double k[2] = {0.0, 0.0}, d[2] = {0.0, 0.0};
+    const int lev[2] = {la, lb};
+    for (int s = 0; s < 2; ++s) {
+        for (int t = __ldg(m.plog_tptr + lev[s]); t < __ldg(m.plog_tptr + lev[s] + 1); ++t) {
+            const double4 c = m.plog_term[t];
+            const double x = c.w * cgm::cg_exp_clamped(arr_ln(c.x, c.y, c.z, pt));
+            k[s] += x;
+            d[s] = fma(x, arr_dln(c.y, c.z, pt), d[s]);
+        }
+        d[s] *= cgm::cg_rcp(k[s]);
+    }
+    if (la == lb) {
+        kf = k[0];
+        dlkf = d[0];
+        dlkf_lnP = 0.0;
+        return;
+    }
+    const double a = __ldg(m.plog_lnp + la), b = __ldg(m.plog_lnp + lb);
+    const double w = (lnP - a) / (b - a);
+    const double kl = cgm::cg_log(k[0]), kh = cgm::cg_log(k[1]);
+    kf = cgm::cg_exp_clamped(kl + (kh - kl) * w);
+    dlkf = fma(w, d[1] - d[0], d[0]);
+    dlkf_lnP = (kh - kl) / (b - a);
+}
+
+// One side of a reaction: species, coefficients (compact or general rows).
+struct Side {
+    int n;
+    int sp[16];
+    double nu[16];
+};
+
+__device__ __forceinline__ void load_sides(const DevMech& m, const DRxn& R, Side& re, Side& pr) {
+    if (R.flags & kFCompact) {
+        re.n = R.nre;
+        pr.n = R.npr;
+        for (int j = 0; j < kMaxCompact; ++j) {
+            re.sp[j] = slot_species(R.sp[j]);
+            re.nu[j] = slot_nu(R.sp[j]);
+            pr.sp[j] = slot_species(R.sp[3 + j]);
+            pr.nu[j] = slot_nu(R.sp[3 + j]);
+        }
+        return;
+    }
+    const int g = R.gen;
+    const int r0 = __ldg(m.gen_rptr + g), r1 = __ldg(m.gen_rptr + g + 1);
+    const int p0 = __ldg(m.gen_pptr + g), p1 = __ldg(m.gen_pptr + g + 1);
+    re.n = min(r1 - r0, 16);
+    pr.n = min(p1 - p0, 16);
+    for (int j = 0; j < re.n; ++j) {
+        re.sp[j] = __ldg(m.gen_sp + r0 + j);
+        re.nu[j] = __ldg(m.gen_nu + r0 + j);
+    }
+    for (int j = 0; j < pr.n; ++j) {
+        pr.sp[j] = __ldg(m.gen_sp + p0 + j);
+        pr.nu[j] = __ldg(m.gen_nu + p0 + j);
+    }
+}
+
+__device__ __forceinline__ double powi(double x, double nu) {
+    if (nu == 1.0) return x;
+    if (nu == 2.0) return x * x;
+    if (nu == 3.0) return x * x * x;
+    return pow(x, nu);
+}
+
+// d(c^nu)/dc
+__device__ __forceinline__ double dpowi(double x, double nu) {
+    if (nu == 1.0) return 1.0;
+    if (nu == 2.0) return 2.0 * x;
+    if (nu == 3.0) return 3.0 * x * x;
+    return nu * pow(x, nu - 1.0);
+}
+
+// Derivative of prod_i c_i^nu_i with respect to factor j (product of the others).
+__device__ __forceinline__ double dprod(const Side& s, const double* c, int j) {
+    double p = dpowi(c[j], s.nu[j]);
+    for (int i = 0; i < s.n; ++i)
+        if (i != j) p *= powi(c[i], s.nu[i]);
+    return p;
+}
+
+template <bool JAC, typename JT>
+__global__ void __launch_bounds__(128) deriv_kernel(DevMech m, const double* __restrict__ P, const double* __restrict__ Tg,
+                                                    const double* __restrict__ Y, const double* __restrict__ G,
+                                                    JT* __restrict__ J, double* __restrict__ gT, double* __restrict__ gY,
+                                                    double* __restrict__ gP, double* __restrict__ scratch, int64_t ng) {
+    const int ns = m.ns;
+    const int64_t ncol = ns + 1;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ng; i += (int64_t)gridDim.x * blockDim.x) {
+        DState st{scratch + i, scratch + (int64_t)ns * ng + i, scratch + (int64_t)2 * ns * ng + i,
+                  scratch + (int64_t)3 * ns * ng + i, ng};
+        const double T = Tg[i], Pv = P[i];
+        PointT pt;
+        pt.T = T;
+        pt.lnT = cgm::cg_log(T);
+        pt.invT = 1.0 / T;
+        double S = 0.0;
+        for (int k = 0; k < ns; ++k) {
+            const double c = Y[(int64_t)k * ng + i] * __ldg(m.inv_mw + k);
+            st.C[k * st.s] = c;
+            S += c;
+        }
+        const double fac = Pv / (kR0 * S * T);
+        double ctot = 0.0;
+        for (int k = 0; k < ns; ++k) {
+            const double c = st.C[k * st.s] * fac;
+            st.C[k * st.s] = c;
+            ctot += c;
+        }
+        const double pfac = kPatm / (kR0 * T);
+        for (int k = 0; k < ns; ++k) {
+            const double* th = m.thermo + 16 * k;
+            const double* c = (T < __ldg(th)) ? th + 1 : th + 8;
+            double cc[7];
+            for (int j = 0; j < 7; ++j) cc[j] = __ldg(c + j);
+            const double smh = smh_poly(cc, T, pt.lnT, pt.invT);
+            st.E[k * st.s] = cgm::cg_exp_clamped(smh) * pfac;
+            // d smh/dT - 1/T
+            const double dp = fma(fma(fma(4.0 * cc[5], T, 3.0 * cc[4]), T, 2.0 * cc[3]), T, cc[2]);
+            st.D[k * st.s] = dp + fma(cc[6], pt.invT, cc[1]) * pt.invT - pt.invT;
+            st.A[k * st.s] = 0.0;
+        }
+        if (JAC) {
+            JT* Jp = J + i;
+            for (int64_t c = 0; c < (int64_t)ns * ncol; ++c) Jp[c * ng] = (JT)0;
+        } else {
+            for (int k = 0; k < ns; ++k) gY[(int64_t)k * ng + i] = 0.0;   // holds C-bar until the end
+        }
+        double tb = 0.0, ab = 0.0, pb = 0.0;
+        const double lnP = cgm::cg_log(Pv);
+        for (int r = 0; r < m.nr; ++r) {
+            const DRxn R = load_rxn(m.rxn + r);
+            int kind = CG_STANDARD;
+            while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
+            Side re, pr;
+            load_sides(m, R, re, pr);
+            double M = 0.0, kf, dlkf, gM = 0.0, dlkf_lnP = 0.0;
+            if (kind != CG_STANDARD && kind != CG_PLOG) {
+                M = ctot;
+                for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
+                    M = fma(__ldg(m.eff_val + e), st.C[__ldg(m.eff_sp + e) * st.s], M);
+            }
+            if (kind == CG_STANDARD || kind == CG_THIRD_BODY) {
+                kf = R.sgn * cgm::cg_exp_clamped(arr_ln(R.lnA, R.b, R.theta, pt));
+                dlkf = arr_dln(R.b, R.theta, pt);
+            } else if (kind == CG_PLOG) {
+                plog_d(m, R.aux, Pv, lnP, pt, kf, dlkf, dlkf_lnP);
+            } else {
+                const DFall f = load_fall(m.fall + R.aux);
+                falloff_d(kind, R.flags, R, f, __ldg(&m.fall2[R.aux].T2), M, pt, kf, dlkf, gM);
+            }
+            double cr[16], cp[16];
+            double pf = 1.0;
+            for (int j = 0; j < re.n; ++j) {
+                cr[j] = st.C[re.sp[j] * st.s];
+                pf *= powi(cr[j], re.nu[j]);
+            }
+            const double qf = kf * pf;
+            double kb = 0.0, qb = 0.0, dlKc = 0.0;
+            if (R.flags & CG_F_REVERSIBLE) {
+                double num = 1.0, den = 1.0, pb_ = 1.0;
+                for (int j = 0; j < re.n; ++j) {
+                    num *= powi(st.E[re.sp[j] * st.s], re.nu[j]);
+                    dlKc = fma(re.nu[j], st.D[re.sp[j] * st.s], dlKc);
+                }
+                for (int j = 0; j < pr.n; ++j) {
+                    cp[j] = st.C[pr.sp[j] * st.s];
+                    den *= powi(st.E[pr.sp[j] * st.s], pr.nu[j]);
+                    pb_ *= powi(cp[j], pr.nu[j]);
+                    dlKc = fma(-pr.nu[j], st.D[pr.sp[j] * st.s], dlKc);
+                }
+                kb = kf * num * cgm::cg_rcp(den);
+                qb = kb * pb_;
+            }
+            const double mfac = (kind == CG_THIRD_BODY) ? M : 1.0;
+            const double dqdT = mfac * fma(qf, dlkf, -qb * (dlkf + dlKc));
+            const double dqdM = (kind == CG_THIRD_BODY) ? (qf - qb) : ((kind >= CG_LINDEMANN && kind <= CG_SRI) ? (qf - qb) * gM : 0.0);
+            const bool usesM = kind >= CG_THIRD_BODY && kind <= CG_SRI;
+            // dq/dC over the reaction's species (reactant slots then product slots)
+            double dqc[32];
+            int dsp[32];
+            int nd = 0;
+            for (int j = 0; j < re.n; ++j) {
+                dsp[nd] = re.sp[j];
+                dqc[nd++] = mfac * kf * dprod(re, cr, j);
+            }
+            if (R.flags & CG_F_REVERSIBLE)
+                for (int j = 0; j < pr.n; ++j) {
+                    dsp[nd] = pr.sp[j];
+                    dqc[nd++] = -mfac * kb * dprod(pr, cp, j);
+                }
+            if (JAC) {
+                JT* Jp = J + i;
+                // rows: every species of the reaction with its net coefficient contribution
+                for (int side = 0; side < 2; ++side) {
+                    const Side& s = side ? pr : re;
+                    const double sg = side ? 1.0 : -1.0;
+                    for (int kk = 0; kk < s.n; ++kk) {
+                        const int k = s.sp[kk];
+                        const double nu = sg * s.nu[kk];
+                        Jp[(int64_t)(k * ncol) * ng] += (JT)(nu * dqdT);
+                        for (int j = 0; j < nd; ++j) Jp[(int64_t)(k * ncol + 1 + dsp[j]) * ng] += (JT)(nu * dqc[j]);
+                        if (usesM) {
+                            st.A[k * st.s] = fma(nu, dqdM, st.A[k * st.s]);
+                            for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
+                                Jp[(int64_t)(k * ncol + 1 + __ldg(m.eff_sp + e)) * ng] +=
+                                    (JT)(nu * __ldg(m.eff_val + e) * dqdM);
+                        }
+                    }
+                }
+            } else {
+                double gq = 0.0;
+                for (int j = 0; j < re.n; ++j) gq = fma(-re.nu[j], G[(int64_t)re.sp[j] * ng + i], gq);
+                for (int j = 0; j < pr.n; ++j) gq = fma(pr.nu[j], G[(int64_t)pr.sp[j] * ng + i], gq);
+                tb = fma(gq, dqdT, tb);
+                for (int j = 0; j < nd; ++j) gY[(int64_t)dsp[j] * ng + i] = fma(gq, dqc[j], gY[(int64_t)dsp[j] * ng + i]);
+                if (usesM) {
+                    ab = fma(gq, dqdM, ab);
+                    for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e) {
+                        const int64_t o = (int64_t)__ldg(m.eff_sp + e) * ng + i;
+                        gY[o] = fma(gq * dqdM, __ldg(m.eff_val + e), gY[o]);
+                    }
+                }
+                if (kind == CG_PLOG) pb = fma(gq, (qf - qb) * dlkf_lnP / Pv, pb);
+            }
+        }
+        const double iS = 1.0 / S;
+        if (JAC) {
+            JT* Jp = J + i;
+            for (int k = 0; k < ns; ++k) {
+                const double ak = st.A[k * st.s];
+                double rk = ak * ctot;
+                for (int j = 0; j < ns; ++j) rk = fma((double)Jp[(int64_t)(k * ncol + 1 + j) * ng], st.C[j * st.s], rk);
+                Jp[(int64_t)(k * ncol) * ng] = (JT)((double)Jp[(int64_t)(k * ncol) * ng] - rk * pt.invT);
+                for (int j = 0; j < ns; ++j) {
+                    const int64_t o = (int64_t)(k * ncol + 1 + j) * ng;
+                    Jp[o] = (JT)(fma(ctot, (double)Jp[o] + ak, -rk) * __ldg(m.inv_mw + j) * iS);
+                }
+            }
+        } else {
+            double rho = 0.0;
+            for (int k = 0; k < ns; ++k) {
+                const double cb = gY[(int64_t)k * ng + i] + ab;
+                gY[(int64_t)k * ng + i] = cb;
+                rho = fma(cb, st.C[k * st.s], rho);
+            }
+            for (int k = 0; k < ns; ++k) {
+                const int64_t o = (int64_t)k * ng + i;
+                gY[o] = fma(ctot, gY[o], -rho) * __ldg(m.inv_mw + k) * iS;
+            }
+            gT[i] = tb - rho * pt.invT;
+            if (gP) gP[i] = fma(rho, 1.0 / Pv, pb);
+        }
+    }
+}
+
+}  // namespace
+
+size_t deriv_workspace_bytes(int ns, int64_t ng) { return (size_t)4 * ns * ng * sizeof(double); }
+
+cudaError_t launch_jacobian(const DevMech& m, int precision, const double* P, const double* T, const double* Y,
+                            void* J, int64_t ng, double* scratch, int sm_count, cudaStream_t s) {
+    if (ng <= 0) return cudaSuccess;
+    int64_t blocks = (ng + 127) / 128;
+    if (blocks > (int64_t)sm_count * 16) blocks = (int64_t)sm_count * 16;
+    if (precision == 0)
+        deriv_kernel<true, double><<<(unsigned)blocks, 128, 0, s>>>(m, P, T, Y, nullptr, (double*)J, nullptr, nullptr,
+                                                                   nullptr, scratch, ng);
+    else
+        deriv_kernel<true, float><<<(unsigned)blocks, 128, 0, s>>>(m, P, T, Y, nullptr, (float*)J, nullptr, nullptr,
+                                                                  nullptr, scratch, ng);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_vjp(const DevMech& m, const double* P, const double* T, const double* Y, const double* G, double* gT,
+                       double* gY, double* gP, int64_t ng, double* scratch, int sm_count, cudaStream_t s) {
+    if (ng <= 0) return cudaSuccess;
+    int64_t blocks = (ng + 127) / 128;
+    if (blocks > (int64_t)sm_count * 16) blocks = (int64_t)sm_count * 16;
+    deriv_kernel<false, double><<<(unsigned)blocks, 128, 0, s>>>(m, P, T, Y, G, nullptr, gT, gY, gP, scratch, ng);
+    return cudaGetLastError();
+}
+
+}  // namespace cg

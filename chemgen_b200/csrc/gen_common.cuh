@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/chemgen_b200.h"
+#include "cg_math.cuh"
 
 namespace cgg {
 
@@ -20,14 +21,7 @@ constexpr double kLog2e = 1.4426950408889634074;
 constexpr double kLn10 = 2.302585092994045684;
 
 // Newton-refined reciprocal (two iterations from the hardware estimate).
-__device__ __forceinline__ double rcp(double x) {
-    double r;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
-    double e = fma(-x, r, 1.0);
-    r = fma(r, e, r);
-    e = fma(-x, r, 1.0);
-    return fma(r, e, r);
-}
+__device__ __forceinline__ double rcp(double x) { return cgm::cg_rcp(x); }
 
 // ---------------------------------------------------------------- mixed
 // 2^a for an FP64 exponent a, returned as FP64 with about 2^-22 relative

@@ -10,7 +10,7 @@
 // reference's device layout (reactions_hip/device_functions_h.j2:701-719), so
 // every per-species load and store of a warp is one contiguous 256-byte run.
 //
-// Per-point state: three arrays of ns doubles -- C (mol/cm^3), EGp = exp(smh) *
+// Per-point state: three arrays of ns doubles -- C (mol/cm^3), EGp = cgm::cg_exp_clamped(smh) *
 // Patm/(R0 T), and the wdot accumulator -- laid out [array][species][thread]
 // in shared memory (ns small enough) or in a per-block slice of a scratch
 // buffer (large ns).  Each thread only ever touches its own column, so the
@@ -23,6 +23,7 @@
 // 16-byte loads.
 #include <cuda_runtime.h>
 
+#include "cg_math.cuh"
 #include "rates_common.cuh"
 
 namespace cg {
@@ -114,7 +115,7 @@ __device__ __forceinline__ void finish(const DevMech& m, const DRxn& R, double k
 }
 
 __device__ __forceinline__ double arrhenius(double lnA, double b, double theta, double sgn, const PointT& pt) {
-    return sgn * exp(fma(b, pt.lnT, lnA) - theta * pt.invT);
+    return sgn * cgm::cg_exp_clamped(fma(b, pt.lnT, lnA) - theta * pt.invT);
 }
 
 template <int B>
@@ -126,7 +127,7 @@ __device__ __forceinline__ double third_body_m(const DevMech& m, int r, double c
 }
 
 // Falloff forward rate: kinf * Pr/(1+Pr) * F (troe.j2:21-45); Lindemann F = 1,
-// SRI F = d [a exp(-b/T) + exp(-T/c)]^X T^e with X = 1/(1 + log10(Pr)^2).
+// SRI F = d [a cgm::cg_exp_clamped(-b/T) + cgm::cg_exp_clamped(-T/c)]^X T^e with X = 1/(1 + cgm::cg_log10(Pr)^2).
 __device__ __forceinline__ double falloff_kf(int kind, int flags, const DRxn& R, const DFall& f, double e_sri_or_t2,
                                              double M, const PointT& pt) {
     const double kinf = arrhenius(R.lnA, R.b, R.theta, R.sgn, pt);
@@ -134,19 +135,19 @@ __device__ __forceinline__ double falloff_kf(int kind, int flags, const DRxn& R,
     const double Pr = k0 * M / kinf;
     double F = 1.0;
     if (kind == CG_TROE) {
-        double Fc = fma(f.p[0], exp(-pt.T * f.p[1]), f.p[2] * exp(-pt.T * f.p[3]));
-        if (flags & CG_F_TROE_T2) Fc += exp(-e_sri_or_t2 * pt.invT);
-        const double lFc = log10(Fc);
+        double Fc = fma(f.p[0], cgm::cg_exp_clamped(-pt.T * f.p[1]), f.p[2] * cgm::cg_exp_clamped(-pt.T * f.p[3]));
+        if (flags & CG_F_TROE_T2) Fc += cgm::cg_exp_clamped(-e_sri_or_t2 * pt.invT);
+        const double lFc = cgm::cg_log10(Fc);
         const double c1 = fma(-0.67, lFc, -0.4);
         const double n1 = fma(-1.27, lFc, 0.75);
-        const double lp = log10(Pr) + c1;
+        const double lp = cgm::cg_log10(Pr) + c1;
         const double f1 = lp / fma(-0.14, lp, n1);
-        F = exp(2.302585092994045684 * lFc / fma(f1, f1, 1.0));
+        F = cgm::cg_exp_clamped(2.302585092994045684 * lFc / fma(f1, f1, 1.0));
     } else if (kind == CG_SRI) {
-        const double lp = log10(Pr);
+        const double lp = cgm::cg_log10(Pr);
         const double X = 1.0 / fma(lp, lp, 1.0);
-        const double base = fma(f.p[0], exp(-f.p[1] * pt.invT), exp(-pt.T * f.p[2]));
-        F = f.p[3] * exp(fma(X, log(base), e_sri_or_t2 * pt.lnT));
+        const double base = fma(f.p[0], cgm::cg_exp_clamped(-f.p[1] * pt.invT), cgm::cg_exp_clamped(-pt.T * f.p[2]));
+        F = f.p[3] * cgm::cg_exp_clamped(fma(X, cgm::cg_log(base), e_sri_or_t2 * pt.lnT));
     }
     return kinf * (Pr / (1.0 + Pr)) * F;
 }
@@ -178,8 +179,8 @@ __device__ __forceinline__ double plog_kf(const DevMech& m, int row, double P, d
         kfh += arrhenius(c.x, c.y, c.z, c.w, pt);
     }
     const double a = __ldg(m.plog_lnp + la), b = __ldg(m.plog_lnp + lb);
-    const double lkl = log(kfl);
-    return exp(lkl + (log(kfh) - lkl) * (lnP - a) / (b - a));
+    const double lkl = cgm::cg_log(kfl);
+    return cgm::cg_exp_clamped(lkl + (cgm::cg_log(kfh) - lkl) * (lnP - a) / (b - a));
 }
 
 // The whole getrates for the point handled by this thread.  `st` points at
@@ -209,12 +210,12 @@ __device__ __forceinline__ void getrates_point(const DevMech& m, bool active, in
     }
     PointT pt;
     pt.T = T;
-    pt.lnT = log(T);
+    pt.lnT = cgm::cg_log(T);
     pt.invT = 1.0 / T;
     // exp_g.j2:2-27, with pfac = Patm/(R0 T) folded in
     const double pfac = kPatm / (kR0 * T);
     for (int k = 0; k < ns; ++k) {
-        st.E[k * B] = exp(species_smh(m.thermo, k, T, pt.lnT, pt.invT)) * pfac;
+        st.E[k * B] = cgm::cg_exp_clamped(species_smh(m.thermo, k, T, pt.lnT, pt.invT)) * pfac;
         st.W[k * B] = 0.0;
     }
     // elementary reactions, two at a time for instruction-level parallelism
@@ -251,7 +252,7 @@ __device__ __forceinline__ void getrates_point(const DevMech& m, bool active, in
     }
     // PLOG
     if (m.seg[CG_PLOG] < m.seg[CG_PLOG + 1]) {
-        const double lnP = log(Pp);
+        const double lnP = cgm::cg_log(Pp);
         for (r = m.seg[CG_PLOG]; r < m.seg[CG_PLOG + 1]; ++r) {
             const DRxn R = load_rxn(m.rxn + r);
             finish<B>(m, R, plog_kf(m, R.aux, Pp, lnP, pt), 1.0, st);

@@ -1,12 +1,12 @@
 // Measurement helpers for the roofline denominators (include/chemgen_b200_probe.h):
 // the FP64 FMA rate of this GPU and the cost, in FP64 FMA issue slots, of
-// the exp / log / reciprocal the kernels use.  Each kernel runs 8
+// the exp / log / reciprocal the kernels use (cg_math.cuh).  Each kernel runs 8
 // independent dependency chains per thread on a grid of many warps, so the
 // timing is throughput-bound.
 #include <cuda_runtime.h>
 
 #include "../../include/chemgen_b200_probe.h"
-#include "rates_common.cuh"
+#include "cg_math.cuh"
 
 namespace {
 
@@ -21,9 +21,9 @@ __global__ void __launch_bounds__(256) probe_kernel(double* out, int iters, doub
 #pragma unroll
         for (int c = 0; c < kChains; ++c) {
             if (OP == 0) x[c] = fma(x[c], 0.999999, 1e-7);
-            if (OP == 1) x[c] = exp(-x[c]);
-            if (OP == 2) x[c] = log(x[c] + 2.0);
-            if (OP == 3) x[c] = cg::rcp_nr(x[c] + 1.0);
+            if (OP == 1) x[c] = cgm::cg_exp(-x[c]);
+            if (OP == 2) x[c] = cgm::cg_log(x[c] + 2.0);
+            if (OP == 3) x[c] = cgm::cg_rcp(x[c] + 1.0);
         }
     }
     double s = 0.0;
@@ -73,4 +73,24 @@ extern "C" int chemgen_probe_fp64(int device, double* fma_tflops, double* exp_fm
     cudaError_t e = cudaGetLastError();
     cudaFree(out);
     return e == cudaSuccess ? 0 : 3;
+}
+
+namespace {
+__global__ void math_check_kernel(const double* x, int n, double* e, double* l, double* er, double* lr) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    e[i] = cgm::cg_exp_clamped(x[i]);
+    er[i] = exp(x[i]);
+    const double y = fabs(x[i]) + 1e-300;
+    l[i] = cgm::cg_log(y);
+    lr[i] = log(y);
+}
+}  // namespace
+
+// Evaluates the kernels' exp/log and CUDA's exp/log on n device values.
+extern "C" int chemgen_probe_math(const double* x, int n, double* exp_out, double* log_out, double* exp_ref,
+                                  double* log_ref) {
+    if (n <= 0) return 0;
+    math_check_kernel<<<(n + 255) / 256, 256>>>(x, n, exp_out, log_out, exp_ref, log_ref);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 3;
 }

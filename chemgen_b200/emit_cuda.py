@@ -32,6 +32,8 @@ LOG10_2 = 0.30102999566398119521
 CSCALE_LOG2 = 32          # mixed: concentrations are stored as C * 2^32 in FP32
 # register-resident wdot accumulators up to this many species
 MAX_REG_SPECIES = 72
+SYNC_EVERY = 8            # reactions between block barriers
+SMEM_BUDGET = 220 * 1024  # dynamic shared memory per block
 
 
 def fingerprint(blob: bytes) -> int:
@@ -57,7 +59,8 @@ def _f(x: float) -> str:
 
 
 class _Emitter:
-    def __init__(self, mech: Mechanism, block: int):
+    def __init__(self, mech: Mechanism, block: int, sync_every: int = 8):
+        self.sync_every = sync_every
         self.mech = mech
         self.ns = mech.ns
         self.idx = mech.species_index()
@@ -116,7 +119,11 @@ class _Emitter:
             parts.append(f"- {_d(th)}*invT")
         if b == 0.0 and th == 0.0:
             return _d(A)
-        return f"{sgn}exp({' '.join(parts)})"
+        # the exponent over 100..10000 K decides whether clamping is needed
+        Ts = [100.0 * 1.1 ** j for j in range(49)]
+        args = [lnA + b * math.log(t) - th / t for t in Ts]
+        fn = "cgm::cg_exp" if -700.0 < min(args) and max(args) < 700.0 else "cgm::cg_exp_clamped"
+        return f"{sgn}{fn}({' '.join(parts)})"
 
     @staticmethod
     def arr2(A: float, b: float, Ea: float) -> Tuple[str, bool]:
@@ -132,30 +139,61 @@ class _Emitter:
         return e, A < 0
 
     # --------------------------------------------------------------- fp64
+    @staticmethod
+    def arg64(A: float, b: float, Ea: float) -> str:
+        """ln|A| + b ln T - Ea/(Rc T) as an FP64 expression."""
+        A, Ea = r15(A), r15(Ea)
+        e = _d(math.log(abs(A)) if A != 0.0 else -745.0)
+        if b != 0.0:
+            e = f"fma({_d(b)}, lnT, {e})"
+        th = Ea / RC_CAL
+        if th != 0.0:
+            e = f"fma({_d(-th)}, invT, {e})"
+        return e
+
     def falloff64(self, r: Reaction) -> List[str]:
+        """kinf * Pr/(1+Pr) * F (troe.j2:21-45) with Pr = exp(ln k0 - ln kinf) M
+        and ln F folded into the exponent of kinf."""
         L = []
-        L.append(f"const double kinf = {self.arr64(*r.arh)};")
-        L.append(f"const double k0 = {self.arr64(*r.low)};")
-        L.append("const double Pr = k0 * M * rcp(kinf);")
+        if r15(r.arh[0]) <= 0.0 or r15(r.low[0]) <= 0.0:
+            # zero or negative pre-exponential factors: direct form
+            L.append(f"const double kinf = {self.arr64(*r.arh)};")
+            L.append(f"const double k0 = {self.arr64(*r.low)};")
+            L.append("const double Pr = k0 * M * rcp(kinf);")
+            L.append("const double lkinf = 0.0;")
+            direct = True
+        else:
+            L.append(f"const double lkinf = {self.arg64(*r.arh)};")
+            L.append(f"const double lr = {self.arg64(*r.low)} - lkinf;")
+            L.append("const double Pr = cgm::cg_exp_clamped(lr) * M;")
+            direct = False
         if r.kind == "troe":
             a, T3, T1 = (r15(x) for x in r.troe[:3])
-            fc = f"fma({_d(r15(1.0 - a))}, exp({_d(-1.0 / T3)}*Tv), {_d(a)}*exp({_d(-1.0 / T1)}*Tv))"
+            fc = (f"fma({_d(r15(1.0 - a))}, cgm::cg_exp_clamped({_d(-1.0 / T3)}*Tv), "
+                  f"{_d(a)}*cgm::cg_exp_clamped({_d(-1.0 / T1)}*Tv))")
             if len(r.troe) == 4 and r.troe[3] != 0.0:
-                fc = f"({fc} + exp({_d(-r15(r.troe[3]))}*invT))"
+                fc = f"({fc} + cgm::cg_exp_clamped({_d(-r15(r.troe[3]))}*invT))"
             L.append(f"const double Fc = {fc};")
-            L.append("const double lFc = log10(Fc);")
-            L.append("const double lp = log10(Pr) + fma(-0.67, lFc, -0.4);")
+            L.append("const double lFc = cgm::cg_log10(Fc);")
+            if direct:
+                L.append("const double lp = cgm::cg_log10(Pr) + fma(-0.67, lFc, -0.4);")
+            else:
+                L.append(f"const double lp = fma(lr, {_d(1.0 / LN10)}, cgm::cg_log10(M)) + fma(-0.67, lFc, -0.4);")
             L.append("const double f1 = lp * rcp(fma(-0.14, lp, fma(-1.27, lFc, 0.75)));")
-            L.append(f"const double F = exp({_d(LN10)} * lFc * rcp(fma(f1, f1, 1.0)));")
+            L.append(f"const double lnF = {_d(LN10)} * lFc * rcp(fma(f1, f1, 1.0));")
         elif r.kind == "sri":
-            s = list(r.sri) + ([1.0, 0.0] if len(r.sri) == 3 else [])
-            L.append("const double lp = log10(Pr);")
+            s_ = list(r.sri) + ([1.0, 0.0] if len(r.sri) == 3 else [])
+            L.append("const double lp = cgm::cg_log10(Pr);")
             L.append("const double X = rcp(fma(lp, lp, 1.0));")
-            L.append(f"const double base = fma({_d(s[0])}, exp({_d(-s[1])}*invT), exp({_d(-1.0 / s[2])}*Tv));")
-            L.append(f"const double F = {_d(s[3])} * exp(fma(X, log(base), {_d(s[4])}*lnT));")
+            L.append(f"const double base = fma({_d(s_[0])}, cgm::cg_exp_clamped({_d(-s_[1])}*invT), "
+                     f"cgm::cg_exp_clamped({_d(-1.0 / s_[2])}*Tv));")
+            L.append(f"const double lnF = {_d(math.log(s_[3]))} + fma(X, cgm::cg_log(base), {_d(s_[4])}*lnT);")
         else:
-            L.append("const double F = 1.0;")
-        L.append("const double kf = kinf * (Pr * rcp(1.0 + Pr)) * F;")
+            L.append("const double lnF = 0.0;")
+        if direct:
+            L.append("const double kf = kinf * (Pr * rcp(1.0 + Pr)) * cgm::cg_exp_clamped(lnF);")
+        else:
+            L.append("const double kf = cgm::cg_exp_clamped(lkinf + lnF) * (Pr * rcp(1.0 + Pr));")
         return L
 
     def plog64(self, r: Reaction) -> List[str]:
@@ -171,8 +209,9 @@ class _Emitter:
         L.append(f"if (Pv < {_d(ps[0])}) {{ kf = {ksum(ps[0])}; }}")
         for lo, hi in zip(ps[:-1], ps[1:]):
             llo, lhi = r15(math.log(lo)), r15(math.log(hi))
-            L.append(f"else if (Pv < {_d(hi)}) {{ const double kl = log({ksum(lo)}); const double kh = log({ksum(hi)}); "
-                     f"kf = exp(kl + (kh - kl) * (lnP - {_d(llo)}) * {_d(1.0 / (lhi - llo))}); }}")
+            L.append(f"else if (Pv < {_d(hi)}) {{ const double kl = cgm::cg_log({ksum(lo)}); "
+                     f"const double kh = cgm::cg_log({ksum(hi)}); "
+                     f"kf = cgm::cg_exp_clamped(kl + (kh - kl) * (lnP - {_d(llo)}) * {_d(1.0 / (lhi - llo))}); }}")
         L.append(f"else {{ kf = {ksum(ps[-1])}; }}")
         return L
 
@@ -339,9 +378,9 @@ class _Emitter:
         L.append("const bool act = i < ng;")
         L.append("const double Tv = act ? T[i] : 1000.0;")
         L.append(f"const double Pv = act ? P[i] : {_d(1013250.0)};")
-        L.append("const double lnT = log(Tv), invT = rcp(Tv);")
+        L.append("const double lnT = cgm::cg_log(Tv), invT = rcp(Tv);")
         if any(r.kind == "plog" for r in self.mech.reactions):
-            L.append("const double lnP = log(Pv);")
+            L.append("const double lnP = cgm::cg_log(Pv);")
         mw = self.mech.mw()
         tmp = "sC" if not mixed else "sG"          # unscaled Y/W, overwritten below
         L.append("double csum = 0.0;")
@@ -372,7 +411,14 @@ class _Emitter:
             poly = (f"fma(fma(fma(fma({sel[5]}, Tv, {sel[4]}), Tv, {sel[3]}), Tv, {sel[2]}), Tv, "
                     f"fma({sel[1]}, lnT, {sel[0]})) - {sel[6]} * invT")
             if not mixed:
-                L.append(f"{{ {pre}sE[{k}][t] = exp({poly}) * pfac; }}")
+                Ts = [200.0 + 50.0 * j for j in range(117)]
+                vals = []
+                for t in Ts:
+                    c = lo if t < sp.t_ranges[1] else hi
+                    vals.append(c[0] + c[1] * math.log(t) + c[2] * t + c[3] * t * t + c[4] * t ** 3
+                                + c[5] * t ** 4 - c[6] / t)
+                fn = "cgm::cg_exp" if max(abs(v) for v in vals) < 690.0 else "cgm::cg_exp_clamped"
+                L.append(f"{{ {pre}sE[{k}][t] = {fn}({poly}) * pfac; }}")
             else:
                 L.append(f"{{ {pre}sG[{k}][t] = fma({poly}, {_d(LOG2E)}, lpfac2); }}")
         if self.reg_w:
@@ -397,7 +443,7 @@ class _Emitter:
     def kernel(self, mixed: bool) -> str:
         ns, B = self.ns, self.block
         name = "cg_gen_mixed" if mixed else "cg_gen_fp64"
-        L = [f"__global__ void __launch_bounds__({B}) {name}(const double* __restrict__ P, "
+        L = [f"__global__ void __launch_bounds__({B}, 1) {name}(const double* __restrict__ P, "
              "const double* __restrict__ T, const double* __restrict__ Y, double* __restrict__ wdot, int64_t ng) {"]
         # dynamic shared memory: [array][species][thread]
         L.append("  extern __shared__ __align__(16) unsigned char dsm[];")
@@ -412,7 +458,11 @@ class _Emitter:
         if not self.reg_w:
             L.append(f"  double (*sW)[{B}] = reinterpret_cast<double (*)[{B}]>(dsm + {off});")
         L += ["  " + x for x in self.prologue(mixed)]
-        for r in self.mech.reactions:
+        for j, r in enumerate(self.mech.reactions):
+            if j and self.sync_every and j % self.sync_every == 0:
+                # keep the block's warps on the same stretch of code so they
+                # share instruction fetches (the kernel is straight-line)
+                L.append("  __syncthreads();")
             L += ["  " + x for x in (self.reaction32(r) if mixed else self.reaction64(r))]
         L += ["  " + x for x in self.epilogue()]
         L.append("}")
@@ -420,20 +470,25 @@ class _Emitter:
 
 
 def choose_block(ns: int) -> int:
-    return 128 if ns <= 24 else 64
+    """One 256-thread block per SM when the per-point state fits (all warps of
+    the SM then walk the code together), else 128."""
+    per = 16 * ns
+    return 256 if 256 * per <= SMEM_BUDGET else 128
 
 
-def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = None) -> str:
+def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = None,
+         sync_every: int = SYNC_EVERY) -> str:
     blob = pack(mech).to_blob()
     fp = fingerprint(blob)
     block = block or choose_block(mech.ns)
-    em = _Emitter(mech, block)
+    em = _Emitter(mech, block, sync_every)
     ident = "".join(ch if ch.isalnum() else "_" for ch in (name or mech.name))
     src = [
         f"// Generated by chemgen_b200 (generate_chemistry.py --language cuda) for mechanism '{mech.name}':",
         f"// {mech.ns} species, {mech.nr} reactions {mech.counts()}.",
         f"// Blob fingerprint 0x{fp:016x}.  Target: sm_100a.",
         '#include "gen_common.cuh"',
+        '#include "cg_math.cuh"',
         "using cgg::rcp;",
         "namespace {",
         em.kernel(False),
@@ -463,6 +518,11 @@ def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = Non
         "}  // namespace",
         "",
         f'extern "C" unsigned long long chemgen_generated_fingerprint_{ident}(void) {{ return 0x{fp:016x}ull; }}',
+        "// direct entry point of this module (the same call chemgen_getrates_ex dispatches to)",
+        f'extern "C" int chemgen_generated_getrates_{ident}(int mode, const double* P, const double* T, int64_t ng,',
+        "                                              const double* Y, double* wdot, void* stream) {",
+        "  return launch(mode, P, T, ng, Y, wdot, stream);",
+        "}",
     ]
     return "\n".join(src) + "\n"
 
@@ -476,14 +536,15 @@ def module_path(mech: Mechanism) -> str:
     return os.path.join(GEN_DIR, f"libcg_{fp:016x}.so")
 
 
-def build_module(mech: Mechanism, out: Optional[str] = None, verbose: bool = False, keep_source: bool = True) -> str:
+def build_module(mech: Mechanism, out: Optional[str] = None, verbose: bool = False, keep_source: bool = True,
+                 **emit_args) -> str:
     """Emit and compile the mechanism's kernels into a shared library that
     links libchemgen_b200.so and registers itself when loaded."""
     from .build import ARCH, FLAGS, OUT as LIBMAIN, nvcc
     os.makedirs(GEN_DIR, exist_ok=True)
     so = out or module_path(mech)
     src = so[:-3] + ".cu"
-    text = emit(mech)
+    text = emit(mech, **emit_args)
     with open(src, "w") as f:
         f.write(text)
     cmd = [nvcc()] + ARCH + FLAGS + ["-I", os.path.join(HERE, "csrc"), "-shared", "-o", so, src,

@@ -59,6 +59,10 @@ def lib() -> ctypes.CDLL:
     L.getrates_hip_wrapper_v1.argtypes = [vp, vp, ci, vp, vp, vp, vp]
     L.getrates_hip_wrapper_v1.restype = None
     L.chemgen_last_wrapper_status.argtypes = []
+    L.chemgen_probe_math.argtypes = [vp, ci, vp, vp, vp, vp]
+    L.chemgen_probe_math.restype = ci
+    L.chemgen_jacobian.argtypes = [vp, ci, vp, vp, i64, vp, vp, vp]
+    L.chemgen_getrates_vjp.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp, vp, vp]
     L.chemgen_use_generated.argtypes = [vp, ci]
     L.chemgen_kernel_kind.argtypes = [vp, ci]
     L.chemgen_register_kernels.argtypes = [ctypes.c_uint64, ci, ci, ctypes.c_uint, vp]
@@ -66,7 +70,7 @@ def lib() -> ctypes.CDLL:
               "chemgen_getrates", "chemgen_getrates_ex", "chemgen_workspace_bytes", "chemgen_getrates_ws",
               "chemgen_getrates_host", "chemgen_init_constants", "chemgen_free_constants",
               "chemgen_last_wrapper_status", "chemgen_use_generated", "chemgen_kernel_kind",
-              "chemgen_register_kernels"):
+              "chemgen_register_kernels", "chemgen_jacobian", "chemgen_getrates_vjp"):
         getattr(L, f).restype = ci
     _lib = L
     return L
@@ -185,6 +189,29 @@ class GpuMechanism:
             out = torch.empty_like(Y)
         self.getrates_ptr(P.data_ptr(), T.data_ptr(), ng, Y.data_ptr(), out.data_ptr(), mode, stream)
         return out
+
+    def jacobian(self, P, T, Y, precision: str = "fp64", out=None, stream=None):
+        """Dense d wdot / d(T, Y): tensor [ns, ns+1, ng] (column 0 = T)."""
+        import torch
+        ns, ng = Y.shape
+        dt = torch.float64 if precision == "fp64" else torch.float32
+        if out is None:
+            out = torch.empty((ns, ns + 1, ng), dtype=dt, device=Y.device)
+        check(lib().chemgen_jacobian(self._h, 0 if precision == "fp64" else 1, P.data_ptr(), T.data_ptr(), ng,
+                                     Y.data_ptr(), out.data_ptr(), _stream(stream)), "chemgen_jacobian")
+        return out
+
+    def vjp(self, P, T, Y, G, stream=None):
+        """(dL/dT [ng], dL/dY [ns, ng], dL/dP [ng]) for G = dL/dwdot [ns, ng]."""
+        import torch
+        ns, ng = Y.shape
+        gT = torch.empty_like(T)
+        gY = torch.empty_like(Y)
+        gP = torch.empty_like(P)
+        check(lib().chemgen_getrates_vjp(self._h, P.data_ptr(), T.data_ptr(), ng, Y.data_ptr(), G.data_ptr(),
+                                         gT.data_ptr(), gY.data_ptr(), gP.data_ptr(), _stream(stream)),
+              "chemgen_getrates_vjp")
+        return gT, gY, gP
 
     def getrates_ws(self, P, T, Y, out, workspace, mode: str = "fp64", stream=None):
         ns, ng = Y.shape

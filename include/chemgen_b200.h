@@ -99,6 +99,20 @@ int chemgen_register_kernels(uint64_t fingerprint, int ns, int nr, unsigned mode
 int chemgen_use_generated(chemgen_handle* h, int enable);
 int chemgen_kernel_kind(chemgen_handle* h, int mode);
 
+/* Analytic derivatives (no counterpart in the reference, whose torch
+ * prototype chemgen/chemistry_nn.py:15-85 never ran); library-owned scratch
+ * of 4*ns*ng doubles.
+ * chemgen_jacobian: dense d wdot/d(T, Y) per point, J[(k*(ns+1) + c)*ng + i],
+ *   column c = 0 for T, 1 + j for Y_j; precision 0 = double, 1 = float
+ *   (FP64 rate evaluation, FP32 accumulation and storage of J).
+ * chemgen_getrates_vjp: given G = dL/dwdot [ns*ng], the adjoint
+ *   gT = dL/dT [ng], gY = dL/dY [ns*ng] and (if gP != NULL) gP = dL/dP [ng],
+ *   without forming J. */
+int chemgen_jacobian(chemgen_handle* h, int precision, const double* P, const double* T, int64_t ng,
+                     const double* Y, void* J, void* stream);
+int chemgen_getrates_vjp(chemgen_handle* h, const double* P, const double* T, int64_t ng, const double* Y,
+                         const double* G, double* gT, double* gY, double* gP, void* stream);
+
 /* Drop-in for the reference's process-global API.
  * chemgen_init_constants replaces copyConstantsToDevice
  * (chemgen/constants.py:119-240): it installs one process-wide mechanism.

@@ -13,6 +13,9 @@
 extern "C" {
 #endif
 int chemgen_probe_fp64(int device, double* fma_tflops, double* exp_fma, double* log_fma, double* rcp_fma);
+/* The kernels' exp (clamped) and log next to CUDA's exp and log(|x|+1e-300)
+ * on n device values; synchronous. */
+int chemgen_probe_math(const double* x, int n, double* exp_out, double* log_out, double* exp_ref, double* log_ref);
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,132 @@
+"""Analytic Jacobian and adjoint kernels against central finite differences
+(h = 1e-6 * max(|x|, floor)) of the FP64 oracle and against torch autograd
+through the FP64 torch restatement of the reference's getrates."""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from chemgen_b200 import pack, synthetic
+from chemgen_b200.runtime import GpuMechanism
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def fd_jacobian(blob, P, T, Y, floor_y=1e-8, rel=1e-6):
+    """Central differences of the oracle: [ns, ns+1, ng]."""
+    ns, ng = Y.shape
+    J = np.empty((ns, ns + 1, ng))
+    h = rel * np.maximum(T, 1.0)
+    wp = oracle.getrates(blob, P, T + h, Y)
+    wm = oracle.getrates(blob, P, T - h, Y)
+    J[:, 0, :] = (wp - wm) / (2 * h)
+    for j in range(ns):
+        h = rel * np.maximum(np.abs(Y[j]), floor_y)
+        Yp, Ym = Y.copy(), Y.copy()
+        Yp[j] += h
+        Ym[j] -= h
+        J[:, 1 + j, :] = (oracle.getrates(blob, P, T, Yp) - oracle.getrates(blob, P, T, Ym)) / (2 * h)
+    return J
+
+
+def _rel(a, b):
+    """max over points of ||a - b|| / ||b|| (Frobenius per point)."""
+    num = np.sqrt(((a - b) ** 2).sum(axis=(0, 1)))
+    den = np.sqrt((b ** 2).sum(axis=(0, 1)))
+    return float((num / den).max())
+
+
+@pytest.mark.parametrize("factory", [synthetic.h2o2_10sp, synthetic.all_kinds, synthetic.gri_shape])
+def test_jacobian_matches_central_differences(factory):
+    mech = factory()
+    blob = pack.pack(mech).to_blob()
+    P, T, Y = synthetic.states(mech.ns, 40, seed=3)
+    Y = np.maximum(Y, 1e-6)
+    Y /= Y.sum(axis=0, keepdims=True)
+    gm = GpuMechanism(blob)
+    J = gm.jacobian(_t(P), _t(T), _t(Y)).cpu().numpy()
+    Jfd = fd_jacobian(blob, P, T, Y)
+    assert _rel(J, Jfd) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["h2_burke", "synthetic_plog_15_40"])
+def test_jacobian_matches_autograd_through_fp64_reference(name):
+    import torch
+    from oracle import torch_ref
+    mech, d = load_golden(name)
+    blob = pack.pack(mech).to_blob()
+    ng = 24
+    P, T, Y = d["P"][:ng], d["T"][:ng], np.ascontiguousarray(d["Y"][:, :ng])
+    gm = GpuMechanism(blob)
+    J = gm.jacobian(_t(P), _t(T), _t(Y)).cpu().numpy()
+    Pt = torch.from_numpy(P)
+    Ja = np.empty_like(J)
+    for i in range(ng):
+        def f(x):
+            return torch_ref.getrates(mech, Pt[i:i + 1], x[:1], x[1:, None])[:, 0]
+        x = torch.cat([torch.from_numpy(T[i:i + 1]), torch.from_numpy(Y[:, i])])
+        Ja[:, :, i] = torch.autograd.functional.jacobian(f, x).numpy()
+    assert _rel(J, Ja) < 1e-9
+
+
+def test_fp32_jacobian_close_to_fp64():
+    mech = synthetic.gri_shape()
+    blob = pack.pack(mech).to_blob()
+    P, T, Y = synthetic.states(mech.ns, 65536, seed=4)
+    gm = GpuMechanism(blob)
+    J64 = gm.jacobian(_t(P), _t(T), _t(Y), "fp64").cpu().numpy()
+    J32 = gm.jacobian(_t(P), _t(T), _t(Y), "fp32").cpu().numpy().astype(np.float64)
+    assert np.all(np.isfinite(J64))
+    assert _rel(J32, J64) < 1e-5
+
+
+def test_vjp_equals_jacobian_transpose_and_autograd_function():
+    import torch
+    from chemgen_b200.autograd import getrates
+    mech = synthetic.all_kinds()
+    blob = pack.pack(mech).to_blob()
+    P, T, Y = synthetic.states(mech.ns, 500, seed=8)
+    gm = GpuMechanism(blob)
+    Pt, Tt, Yt = _t(P), _t(T), _t(Y)
+    G = torch.randn(mech.ns, 500, dtype=torch.float64, device="cuda")
+    J = gm.jacobian(Pt, Tt, Yt)
+    gT, gY, gP = gm.vjp(Pt, Tt, Yt, G)
+    ref_T = (J[:, 0, :] * G).sum(0)
+    ref_Y = torch.einsum("kjn,kn->jn", J[:, 1:, :], G)
+    assert torch.allclose(gT, ref_T, rtol=1e-9, atol=1e-9 * ref_T.abs().max().item())
+    assert torch.allclose(gY, ref_Y, rtol=1e-9, atol=1e-9 * ref_Y.abs().max().item())
+    # dL/dP against central differences of the forward kernel
+    h = 1e-6 * Pt
+    wp = gm.getrates(Pt + h, Tt, Yt)
+    wm = gm.getrates(Pt - h, Tt, Yt)
+    fdP = ((wp - wm) * G).sum(0) / (2 * h)
+    assert torch.allclose(gP, fdP, rtol=1e-5, atol=1e-6 * fdP.abs().max().item())
+    # autograd.Function: backward is the adjoint kernel
+    Tr, Yr = Tt.clone().requires_grad_(True), Yt.clone().requires_grad_(True)
+    w = getrates(gm, Pt, Tr, Yr)
+    (w * G).sum().backward()
+    assert torch.allclose(Tr.grad, gT) and torch.allclose(Yr.grad, gY)
+
+
+def test_jacobian_with_zero_species_is_exact():
+    """Y_j = 0 exactly: the analytic derivative must not vanish where FD says it doesn't."""
+    import torch
+    from oracle import torch_ref
+    mech = synthetic.h2o2_10sp()
+    blob = pack.pack(mech).to_blob()
+    P, T, Y = synthetic.states(mech.ns, 8, seed=2)
+    Y[3, :] = 0.0
+    Y /= Y.sum(axis=0, keepdims=True)
+    J = GpuMechanism(blob).jacobian(_t(P), _t(T), _t(Y)).cpu().numpy()
+    for i in range(8):
+        def f(x):
+            return torch_ref.getrates(mech, torch.from_numpy(P[i:i + 1]), x[:1], x[1:, None])[:, 0]
+        x = torch.cat([torch.from_numpy(T[i:i + 1]), torch.from_numpy(Y[:, i])])
+        Ja = torch.autograd.functional.jacobian(f, x).numpy()
+        assert np.abs(J[:, :, i] - Ja).max() <= 1e-9 * np.abs(Ja).max()
+        assert np.abs(J[:, 4, i]).max() > 0      # column of the absent species

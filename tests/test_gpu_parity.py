@@ -163,3 +163,25 @@ def test_bad_arguments_return_status():
         gm.getrates_ptr(x.data_ptr() + 4, x.data_ptr(), 1, x.data_ptr(), x.data_ptr())
     with pytest.raises(ChemgenError):
         gm.getrates_ptr(x.data_ptr(), x.data_ptr(), -1, x.data_ptr(), x.data_ptr())
+
+
+def test_kernel_exp_log_against_cuda_libm():
+    import torch
+    from chemgen_b200.runtime import lib
+    rng = np.random.default_rng(0)
+    x = np.concatenate([rng.uniform(-740, 705, 200000), rng.uniform(-1, 1, 100000),
+                        np.exp(rng.uniform(-700, 700, 100000)), [0.0, -0.0, 1.0, 2.0, 700.0, -708.0]])
+    xt = torch.from_numpy(x).cuda()
+    outs = [torch.empty_like(xt) for _ in range(4)]
+    assert lib().chemgen_probe_math(ctypes_ptr(xt), x.size, *(ctypes_ptr(o) for o in outs)) == 0
+    e, l, er, lr = (o.cpu().numpy() for o in outs)
+    ok = (er > 1e-300) & np.isfinite(er)
+    assert np.max(np.abs(e[ok] - er[ok]) / er[ok]) < 1e-15
+    assert np.all(np.isinf(e[np.isinf(er)]))
+    ok = np.abs(lr) > 1e-3
+    assert np.max(np.abs(l[ok] - lr[ok]) / np.abs(lr[ok])) < 1e-15
+    assert np.max(np.abs(l - lr)) < 1e-15 * 800
+
+
+def ctypes_ptr(t):
+    return t.data_ptr()
