@@ -400,6 +400,8 @@ int run_owned(chemgen_handle* h, int mode, const double* P, const double* T, int
 
 std::mutex g_mu;
 chemgen_handle* g_handle = nullptr;
+
+
 int g_wrapper_status = CHEMGEN_OK;
 
 }  // namespace

@@ -137,7 +137,7 @@ class Mechanism:
 
     # ------------------------------------------------------------------ json
     def to_json(self) -> str:
-        return json.dumps(dataclasses.asdict(self), sort_keys=True)
+        return json.dumps(dataclasses.asdict(self))
 
     @staticmethod
     def from_json(text: str) -> "Mechanism":

@@ -1,0 +1,45 @@
+"""The generator CLI: --mode getrates --language cuda emits compilable
+sm_100a source and the blob the C ABI loads."""
+import os
+import subprocess
+import sys
+
+import pytest
+
+from conftest import REPO, REFERENCE, reference_available
+from chemgen_b200 import pack, synthetic
+from oracle import oracle
+
+
+def test_blob_mode_roundtrip(tmp_path):
+    yaml_path = tmp_path / "mech.yaml"
+    out = tmp_path / "mech.blob"
+    # a mechanism file written from the package's own JSON form
+    mech = synthetic.h2o2_10sp()
+    (tmp_path / "mech.json").write_text(mech.to_json())
+    r = subprocess.run([sys.executable, os.path.join(REPO, "generate_chemistry.py"), "--mode", "blob",
+                        "--mech", str(tmp_path / "mech.json"), "--output", str(out)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert out.read_bytes() == pack.pack(mech).to_blob()
+    assert oracle.check_blob(out.read_bytes()) == 0
+
+
+@pytest.mark.skipif(not reference_available(), reason="reference mechanism files not present")
+@pytest.mark.parametrize("src", [("GRI30/chem.inp", "GRI30/therm.dat"), ("H2_burke/chem.yaml", None)])
+def test_getrates_cuda_emits_compilable_source(tmp_path, src):
+    mech_file, therm = src
+    out = tmp_path / "getrates.cu"
+    cmd = [sys.executable, os.path.join(REPO, "generate_chemistry.py"), "--mode", "getrates", "--language", "cuda",
+           "--mech", os.path.join(REFERENCE, "ck_files", mech_file), "--output", str(out)]
+    if therm:
+        cmd += ["--therm", os.path.join(REFERENCE, "ck_files", therm)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    text = out.read_text()
+    assert "__global__" in text and "cg_gen_fp64" in text and "cg_gen_mixed" in text
+    assert oracle.check_blob((tmp_path / "getrates.blob").read_bytes()) == 0
+    from chemgen_b200.build import ARCH, FLAGS, nvcc
+    obj = tmp_path / "g.o"
+    r = subprocess.run([nvcc()] + ARCH + FLAGS + ["-I", os.path.join(REPO, "chemgen_b200", "csrc"), "-c",
+                        str(out), "-o", str(obj)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
