@@ -401,7 +401,18 @@ int run_owned(chemgen_handle* h, int mode, const double* P, const double* T, int
 std::mutex g_mu;
 chemgen_handle* g_handle = nullptr;
 
+}  // namespace
 
+namespace cg {
+// Read-only view of a handle for the other translation units of the library.
+const DevMech* handle_mech(const chemgen_handle* h, int* device, int64_t* max_slices) {
+    if (device) *device = h->device;
+    if (max_slices) *max_slices = h->fp64_slices;
+    return &h->m;
+}
+}  // namespace cg
+
+namespace {
 int g_wrapper_status = CHEMGEN_OK;
 
 }  // namespace

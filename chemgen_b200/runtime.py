@@ -63,6 +63,8 @@ def lib() -> ctypes.CDLL:
     L.chemgen_probe_math.restype = ci
     L.chemgen_jacobian.argtypes = [vp, ci, vp, vp, i64, vp, vp, vp]
     L.chemgen_getrates_vjp.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp, vp, vp]
+    L.chemgen_getrates_noalloc.argtypes = [vp, vp, vp, i64, vp, vp, vp]
+    L.chemgen_getrates_noalloc.restype = ci
     L.chemgen_use_generated.argtypes = [vp, ci]
     L.chemgen_kernel_kind.argtypes = [vp, ci]
     L.chemgen_register_kernels.argtypes = [ctypes.c_uint64, ci, ci, ctypes.c_uint, vp]

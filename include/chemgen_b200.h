@@ -113,6 +113,21 @@ int chemgen_jacobian(chemgen_handle* h, int precision, const double* P, const do
 int chemgen_getrates_vjp(chemgen_handle* h, const double* P, const double* T, int64_t ng, const double* Y,
                          const double* G, double* gT, double* gY, double* gP, void* stream);
 
+/* FP64 getrates that allocates no device memory (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc while they run -- a
+ * solver that owns the device memory pool or forbids allocation (and the
+ * device synchronisation cudaMalloc/cudaFree can cause) inside its time-step
+ * loop.  The per-point state that the large-mechanism FP64 kernel keeps in
+ * scratch lives in a fixed 16 MiB device array inside the library (held on
+ * every GPU that loads it until exit) instead of a library allocation.
+ * Device pointers and layouts as chemgen_getrates.  A mechanism whose state
+ * slice of 3*ns*64 doubles exceeds the array (ns > 10922) returns
+ * CHEMGEN_ERR_TOO_LARGE.  The first call on a device looks up the array's
+ * address (with that device current): make it before any stream capture.
+ * All calls share the array, so calls that overlap on the GPU race. */
+int chemgen_getrates_noalloc(chemgen_handle* h, const double* P, const double* T, int64_t ng, const double* Y,
+                             double* wdot, void* stream);
+
 /* Drop-in for the reference's process-global API.
  * chemgen_init_constants replaces copyConstantsToDevice
  * (chemgen/constants.py:119-240): it installs one process-wide mechanism.
