@@ -94,3 +94,65 @@ extern "C" int chemgen_probe_math(const double* x, int n, double* exp_out, doubl
     math_check_kernel<<<(n + 255) / 256, 256>>>(x, n, exp_out, log_out, exp_ref, log_ref);
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : 3;
 }
+
+// ---------------------------------------------------------------------------
+// Self-check of the tcgen05 building blocks (umma.cuh): one CTA computes
+// D[128 x N] = A[128 x K] * B[N x K]^T, BF16 in, FP32 out.
+#include "umma.cuh"
+
+namespace {
+__global__ void __launch_bounds__(128) umma_probe_kernel(const __nv_bfloat16* A, const __nv_bfloat16* B, float* D,
+                                                         int N, int K, uint32_t ncols, int* err) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    unsigned char* sA = sm;
+    unsigned char* sB = sm + 128 * K * 2;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(sB + N * K * 2);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int idx = tid; idx < 128 * K; idx += 128)
+        *reinterpret_cast<__nv_bfloat16*>(sA + um::kmajor_offset(idx / K, idx % K, K)) = A[idx];
+    for (int idx = tid; idx < N * K; idx += 128)
+        *reinterpret_cast<__nv_bfloat16*>(sB + um::kmajor_offset(idx / K, idx % K, K)) = B[idx];
+    if (tid == 0) {
+        um::mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) um::tmem_alloc(tslot, ncols);
+    um::fence_proxy_async();
+    um::fence_before_sync();
+    __syncthreads();
+    um::fence_after_sync();
+    const uint32_t taddr = *tslot;
+    if (tid == 0) {
+        const uint32_t idesc = um::idesc_bf16(128, N);
+        const uint32_t a0 = um::smem_addr(sA), b0 = um::smem_addr(sB);
+        for (int s = 0; s < K / 16; ++s)
+            um::mma_bf16(taddr, um::desc_kmajor(a0, K, s), um::desc_kmajor(b0, K, s), idesc, s > 0 ? 1u : 0u);
+        um::commit(mbar);
+    }
+    const bool ok = um::mbar_wait(mbar, 0);
+    if (!ok && lane == 0) atomicExch(err, 1);
+    um::fence_after_sync();
+    if (ok) {
+        for (int c = 0; c < N; c += 16) {
+            float v[16];
+            um::tmem_ld16(um::tmem_lane_addr(taddr, warp, c), v);
+            for (int j = 0; j < 16; ++j) D[(32 * warp + lane) * N + c + j] = v[j];
+        }
+    }
+    um::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) um::tmem_dealloc(taddr, ncols);
+}
+}  // namespace
+
+extern "C" int chemgen_probe_umma(const void* A, const void* B, float* D, int N, int K, int* err) {
+    if (N < 16 || N > 256 || N % 16 || K < 16 || K > 256 || K % 16 || !A || !B || !D || !err) return 1;
+    uint32_t ncols = 32;
+    while ((int)ncols < N) ncols <<= 1;
+    const size_t smem = (size_t)(128 + N) * K * 2 + 16;
+    if (cudaFuncSetAttribute(umma_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 3;
+    umma_probe_kernel<<<1, 128, smem>>>((const __nv_bfloat16*)A, (const __nv_bfloat16*)B, D, N, K, ncols, err);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 3;
+}

@@ -1,0 +1,124 @@
+// tcgen05 (5th-generation tensor core) building blocks for sm_100a:
+// D[128 x N] (FP32, in tensor memory) += A[128 x K] * B[N x K]^T with BF16
+// A and B staged in shared memory in the K-major, no-swizzle canonical
+// layout.
+//
+// Shared-memory operand layout ("core matrices" of 8 rows x 16 bytes): element
+// (r, k) of an [R x K] BF16 tile sits at byte
+//     (r / 8) * (K * 16) + (k / 8) * 128 + (r % 8) * 16 + (k % 8) * 2,
+// i.e. the two 16-byte K chunks of one 16-wide MMA step are 128 bytes apart
+// (leading byte offset) and consecutive 8-row groups are K*16 bytes apart
+// (stride byte offset).  The matrix descriptor fields (start address, LBO,
+// SBO in 16-byte units, version 1 at bit 46, layout type 0 at bits 61-63) and
+// the instruction descriptor fields (D format bits 4-5, A/B format bits 7-9 /
+// 10-12, N/8 at bits 17-22, M/16 at bits 24-28) follow the PTX ISA's
+// tcgen05 matrix and instruction descriptor formats.
+//
+// Every wait on an mbarrier is bounded; on time-out the caller's error word is
+// set and the kernel proceeds to free its tensor memory.
+#pragma once
+
+#include <cstdint>
+#include <cuda_bf16.h>
+
+namespace um {
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint32_t kmajor_offset(int r, int k, int K) {
+    return (uint32_t)((r >> 3) * (K * 16) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// Matrix descriptor of the K-major tile at `saddr` (16-byte aligned), K
+// elements per row, positioned at MMA step `kstep` (16 elements per step).
+__device__ __forceinline__ uint64_t desc_kmajor(uint32_t saddr, int K, int kstep) {
+    const uint32_t start = saddr + (uint32_t)kstep * 256u;
+    const uint64_t lbo = 128u >> 4;
+    const uint64_t sbo = (uint64_t)(K * 16) >> 4;
+    return (uint64_t)((start >> 4) & 0x3fffu) | (lbo << 16) | (sbo << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: BF16 A and B (K-major), FP32 D, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+        "}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void commit(uint64_t* mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_addr(mbar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(mbar)), "r"(count) : "memory");
+}
+
+// Bounded wait for phase `parity`; returns false on time-out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t max_iters = (1u << 24)) {
+    const uint32_t a = smem_addr(mbar);
+    for (uint32_t it = 0; it < max_iters; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t"
+            ".reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t"
+            "}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Warp-wide (one full warp): allocate `ncols` (power of two >= 32) TMEM
+// columns; the base address is written to *dst (shared memory).
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(dst)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32  %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane (warp w reads lanes 32w..32w+31).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32"
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ uint32_t tmem_lane_addr(uint32_t base, int warp_in_group, int col) {
+    return base + ((uint32_t)(32 * warp_in_group) << 16) + (uint32_t)col;
+}
+
+}  // namespace um

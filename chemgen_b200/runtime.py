@@ -61,6 +61,8 @@ def lib() -> ctypes.CDLL:
     L.chemgen_last_wrapper_status.argtypes = []
     L.chemgen_probe_math.argtypes = [vp, ci, vp, vp, vp, vp]
     L.chemgen_probe_math.restype = ci
+    L.chemgen_probe_umma.argtypes = [vp, vp, vp, ci, ci, vp]
+    L.chemgen_probe_umma.restype = ci
     L.chemgen_jacobian.argtypes = [vp, ci, vp, vp, i64, vp, vp, vp]
     L.chemgen_getrates_vjp.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp, vp, vp]
     L.chemgen_getrates_noalloc.argtypes = [vp, vp, vp, i64, vp, vp, vp]
