@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--ng", type=int, default=1 << 20)
-    ap.add_argument("--modes", default="fp64,mixed")
+    ap.add_argument("--modes", default="fp64,mixed,mixed_tc")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--clock-ms", type=float, default=1500.0, help="length of the clock-sampled timed pass")
     ap.add_argument("--e2e-steps", type=int, default=-1, help="host-path steps (default min(steps, 50))")
@@ -197,6 +197,9 @@ def run_ours(args, rank, world, local_rank):
     W = torch.empty_like(Yd)
     stream = torch.cuda.current_stream()
 
+    # the table-driven tensor-core mixed kernel on its own handle
+    gm_tc = GpuMechanism(blob, device=local_rank)
+    gm_tc.use_generated(False)
     modes = []
     for m in args.modes.split(","):
         try:
@@ -215,15 +218,23 @@ def run_ours(args, rank, world, local_rank):
     bytes_pt = ops.bytes_per_point(mech.ns)
     hbm_peak, hbm_src = measured_peaks()
 
+    def runner(m):
+        if m == "mixed_tc":
+            return lambda: gm_tc.getrates(Pd, Td, Yd, out=W, mode="mixed", stream=stream)
+        return lambda: gm.getrates(Pd, Td, Yd, out=W, mode=m, stream=stream)
+
+    if "mixed_tc" in args.modes.split(",") and gm_tc.kernel_kind("mixed") == "table":
+        modes.append("mixed_tc")
     results = {}
     for m in modes:
-        fn = lambda m=m: gm.getrates(Pd, Td, Yd, out=W, mode=m, stream=stream)
+        fn = runner(m)
         ms = time_steps(fn, args.steps, args.warmup, stream)
         if world > 1:
             t = torch.tensor([ms], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
-        results[m] = {"ms_per_step": ms, "value": ng * world / (ms * 1e-3) / 1e6, "kernel": gm.kernel_kind(m)}
+        kind = gm_tc.kernel_kind("mixed") + "-tensorcore" if m == "mixed_tc" else gm.kernel_kind(m)
+        results[m] = {"ms_per_step": ms, "value": ng * world / (ms * 1e-3) / 1e6, "kernel": kind}
 
     # errors and CPU baseline on a bounded sample (rank 0, single GPU)
     err = {}
@@ -248,7 +259,7 @@ def run_ours(args, rank, world, local_rank):
                          f"generated getrates, OpenMP over points ({dt:.1f} s)"}
         idx_t = torch.from_numpy(idx).to(dev)
         for m in modes:
-            gm.getrates(Pd, Td, Yd, out=W, mode=m, stream=stream)
+            runner(m)()
             w = W.index_select(1, idx_t).cpu().numpy()
             S = r["S"] if r is not None else None
             err[m] = oracle.errors(w, w_ref, S)
@@ -259,7 +270,7 @@ def run_ours(args, rank, world, local_rank):
 
     # clocks during a timed pass of the headline mode
     sampler = ClockSampler(local_rank)
-    fn = lambda: gm.getrates(Pd, Td, Yd, out=W, mode=head, stream=stream)
+    fn = runner(head)
     steps_c = max(args.steps, int(math.ceil(args.clock_ms / max(results[head]["ms_per_step"], 1e-3))))
     with sampler:
         ms_c = time_steps(fn, steps_c, 2, stream)
@@ -269,14 +280,16 @@ def run_ours(args, rank, world, local_rank):
     # end to end through the host-pointer API: pinned inputs in, wdot back on the host
     Ph, Th, Yh = (torch.from_numpy(x).pin_memory() for x in (P, T, Y))
     Wh = torch.empty_like(Yh).pin_memory()
+    gm_e2e = gm_tc if head == "mixed_tc" else gm
+    mode_e2e = "mixed" if head == "mixed_tc" else head
     for _ in range(2):
-        gm.getrates_host(Ph, Th, Yh, out=Wh.numpy(), mode=head)
+        gm_e2e.getrates_host(Ph, Th, Yh, out=Wh.numpy(), mode=mode_e2e)
     k_e2e = max(1, min(args.steps, 50)) if args.e2e_steps < 0 else args.e2e_steps
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(k_e2e):
-        gm.getrates_host(Ph, Th, Yh, out=Wh.numpy(), mode=head)
+        gm_e2e.getrates_host(Ph, Th, Yh, out=Wh.numpy(), mode=mode_e2e)
     e2e_s = (time.perf_counter() - t0) / max(k_e2e, 1)
     if world > 1:
         t = torch.tensor([e2e_s], device=dev)

@@ -1,0 +1,532 @@
+// Mixed-precision getrates with the stoichiometric contraction on the
+// 5th-generation tensor cores (tcgen05).  Table-driven: one compiled kernel
+// serves every mechanism loaded at run time, including 348-species /
+// 2163-reaction ones.
+//
+// Work split.  A CTA owns a tile of 128 grid points -- one point per thread,
+// one point per TMEM lane.  For every chunk of 16 reactions each thread
+// computes its point's net rates of progress q (the reference's
+// rr = kf prod C^nu - kb prod C^nu, reactions/standard.j2:3-19, with the
+// third-body factor of third_body.j2:30 and the falloff of troe.j2:9-45)
+// and writes them, split exactly into three BF16 parts q = q_hi + q_mid +
+// q_lo, into shared memory as the A operand of an MMA whose B operand is
+// the chunk's net stoichiometric matrix nu (exact in BF16).  One thread
+// issues tcgen05.mma; the products accumulate in FP32 in tensor memory,
+// D[point][species] = sum_r q_r nu_rk, which is wdot
+// (reactions/standard.j2:21-27).  Two chunk buffers let the tensor core
+// accumulate one chunk while the threads compute the next.
+//
+// Arithmetic.  Exponents are formed in FP64: ln A + b ln T - Ea/(Rc T) and
+// the Gibbs sums sum nu G that give Kc (G = log2(exp(smh) Patm/(R0 T))).
+// 2^f of the fractional part runs on the SFU (ex2.approx.f32); concentration
+// products are FP32 on C * 2^32 (so that they stay clear of FP32 underflow);
+// q is FP32 and the accumulation FP32.  PLOG reactions and reactions with
+// fractional stoichiometry are evaluated in FP64 and rounded to FP32.
+//
+// Per-point state: C (FP32, shared memory) and G (FP64, shared memory, or a
+// per-CTA slice of global scratch when the mechanism is too large).
+// Every mbarrier wait is bounded; a time-out sets the error word.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "cg_math.cuh"
+#include "gen_common.cuh"
+#include "rates_common.cuh"
+#include "umma.cuh"
+
+namespace cg {
+
+constexpr int kTile = 128;       // points per CTA tile (TMEM lanes)
+constexpr int kChunk = 16;       // reactions per MMA chunk (MMA K)
+constexpr int kABytes = kTile * kChunk * 2;   // one BF16 A split tile
+
+struct MixedPlan {
+    int ns = 0, nr = 0, npad = 0, nhalf = 0, nchunk = 0;
+    uint32_t tcols = 0;
+    int g_smem = 0;
+    size_t smem = 0;
+    int grid = 0;
+    int group = 4;          // chunks accumulated in FP32 before the FP64 flush
+    void* dbuf = nullptr;
+    const __nv_bfloat16* nu = nullptr;
+    int* err = nullptr;
+};
+
+namespace {
+
+constexpr double kLog2eD = 1.4426950408889634074;
+constexpr float kLog2eF = 1.44269504f;
+constexpr float kLog10_2F = 0.30103000f;
+
+// 2^e for an integer e, applied in two FP32 steps so that large products
+// with small scales (and the reverse) keep their value.
+__device__ __forceinline__ float scale2(float m, int e) {
+    const int e1 = max(-126, min(e, 127));
+    const int e2 = max(-126, min(e - e1, 127));
+    return m * __int_as_float((e1 + 127) << 23) * __int_as_float((e2 + 127) << 23);
+}
+
+// FP32 q = 2^a * prod * 2^eoff, a in FP64.
+__device__ __forceinline__ float rate32(double a, float prod, int eoff) {
+    const double magic = 6755399441055744.0;
+    const double t = a + magic;
+    const int n = __double2loint(t);
+    const float f = (float)(a - (t - magic));
+    return scale2(cgg::ex2f(f) * prod, n + eoff);
+}
+
+struct TileCtx {
+    const float* C;      // C * 2^32, stride kTile
+    const double* G;     // log2 Gibbs terms, stride kTile
+    double T, Pv, lnT, lnT2, invT;
+    float ctot32, Tf, invTf, lnT2f;
+};
+
+// log2 kf of a falloff reaction (Lindemann, Troe, SRI): FP64 exponents, FP32 blending.
+__device__ double falloff_l2(int kind, int flags, const DRxn& R, const DFall& f, double x2, float Ms,
+                             const TileCtx& c) {
+    const double ainf = (fma(R.b, c.lnT, R.lnA) - R.theta * c.invT) * kLog2eD;
+    const double a0 = (fma(f.b0, c.lnT, f.lnA0) - f.theta0 * c.invT) * kLog2eD;
+    const double d = a0 - ainf;
+    const double magic = 6755399441055744.0;
+    const double t = d + magic;
+    int npr = __double2loint(t);
+    float mpr = cgg::ex2f((float)(d - (t - magic))) * Ms;
+    const int ex = ((__float_as_int(mpr) >> 23) & 0xff) - 126;
+    npr += ex - 32;
+    mpr = __int_as_float((__float_as_int(mpr) & 0x807fffff) | (126 << 23));   // [0.5, 1)
+    const float l2pr = (float)npr + cgg::lg2f(mpr);
+    float l2r;
+    int nfix = 0;
+    if (npr < 0) {
+        const float pr = npr > -126 ? ldexpf(mpr, npr) : 0.0f;
+        l2r = cgg::lg2f(mpr) - cgg::lg2f(1.0f + pr);
+        nfix = npr;
+    } else {
+        const float ipr = npr < 126 ? ldexpf(1.0f / mpr, -npr) : 0.0f;
+        l2r = -cgg::lg2f(1.0f + ipr);
+    }
+    float l2F = 0.0f;
+    if (kind == CG_TROE) {
+        float Fc = fmaf((float)f.p[0], cgg::ex2f(-kLog2eF * c.Tf * (float)f.p[1]),
+                        (float)f.p[2] * cgg::ex2f(-kLog2eF * c.Tf * (float)f.p[3]));
+        if (flags & CG_F_TROE_T2) Fc += cgg::ex2f(-kLog2eF * (float)x2 * c.invTf);
+        const float lFc = kLog10_2F * cgg::lg2f(Fc);
+        const float lp = kLog10_2F * l2pr + fmaf(-0.67f, lFc, -0.4f);
+        const float f1 = __fdividef(lp, fmaf(-0.14f, lp, fmaf(-1.27f, lFc, 0.75f)));
+        l2F = __fdividef(lFc, fmaf(f1, f1, 1.0f)) / kLog10_2F;
+    } else if (kind == CG_SRI) {
+        const float lp = kLog10_2F * l2pr;
+        const float X = __fdividef(1.0f, fmaf(lp, lp, 1.0f));
+        const float base = fmaf((float)f.p[0], cgg::ex2f(-kLog2eF * (float)f.p[1] * c.invTf),
+                                cgg::ex2f(-kLog2eF * c.Tf * (float)f.p[2]));
+        l2F = cgg::lg2f((float)f.p[3]) + fmaf(X, cgg::lg2f(base), (float)x2 * c.lnT2f);
+    }
+    return ainf + ((double)nfix + (double)(l2r + l2F));
+}
+
+// PLOG forward rate in FP64 (plog.j2:4-38).
+__device__ double plog_kf64(const DevMech& m, int row, double P, double lnT, double invT) {
+    const int l0 = __ldg(m.plog_ptr + row), l1 = __ldg(m.plog_ptr + row + 1);
+    int l = l0;
+    while (l < l1 && !(P < __ldg(m.plog_p + l))) ++l;
+    int la, lb;
+    if (l == l0) la = lb = l0;
+    else if (l == l1) la = lb = l1 - 1;
+    else {
+        la = l - 1;
+        lb = l;
+    }
+    double k[2] = {0.0, 0.0};
+    const int lev[2] = {la, lb};
+    for (int s = 0; s < (la == lb ? 1 : 2); ++s)
+        for (int t = __ldg(m.plog_tptr + lev[s]); t < __ldg(m.plog_tptr + lev[s] + 1); ++t) {
+            const double4 cc = m.plog_term[t];
+            k[s] += cc.w * cgm::cg_exp_clamped(fma(cc.y, lnT, cc.x) - cc.z * invT);
+        }
+    if (la == lb) return k[0];
+    const double a = __ldg(m.plog_lnp + la), b = __ldg(m.plog_lnp + lb);
+    const double kl = cgm::cg_log(k[0]);
+    return cgm::cg_exp_clamped(kl + (cgm::cg_log(k[1]) - kl) * (cgm::cg_log(P) - a) / (b - a));
+}
+
+// Net rate of progress of reaction r at this thread's point, FP32.
+__device__ float rate_of_progress(const DevMech& m, int r, const TileCtx& c, int tid) {
+    const DRxn R = load_rxn(m.rxn + r);
+    int kind = CG_STANDARD;
+    while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
+    float Ms = 0.0f;
+    if (kind >= CG_THIRD_BODY && kind <= CG_SRI) {
+        Ms = c.ctot32;
+        for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
+            Ms = fmaf((float)__ldg(m.eff_val + e), c.C[__ldg(m.eff_sp + e) * kTile + tid], Ms);
+    }
+    const bool compact = (R.flags & kFCompact) != 0;
+    const bool neg_falloff = kind >= CG_LINDEMANN && kind <= CG_SRI && (R.flags & (CG_F_A_NEG | CG_F_LOW_NEG));
+    if (!compact || kind == CG_PLOG || neg_falloff) {
+        // FP64 evaluation of this reaction
+        double kf;
+        if (kind == CG_PLOG) kf = plog_kf64(m, R.aux, c.Pv, c.lnT, c.invT);
+        else if (kind <= CG_THIRD_BODY) kf = R.sgn * cgm::cg_exp_clamped(fma(R.b, c.lnT, R.lnA) - R.theta * c.invT);
+        else {
+            const DFall f = load_fall(m.fall + R.aux);
+            kf = R.sgn * exp2(falloff_l2(kind, R.flags, R, f, __ldg(&m.fall2[R.aux].T2), Ms, c));
+        }
+        const double cs = 2.3283064365386963e-10;   // 2^-32
+        double qf = kf, qb = 0.0, g = 0.0;
+        {
+            if (compact) {
+                for (int j = 0; j < R.nre; ++j) {
+                    const int s = slot_species(R.sp[j]);
+                    qf *= ipow3((double)c.C[s * kTile + tid] * cs, slot_nu(R.sp[j]));
+                    g = fma((double)slot_nu(R.sp[j]), c.G[s * kTile + tid], g);
+                }
+                double pb = 1.0;
+                for (int j = 0; j < R.npr; ++j) {
+                    const int s = slot_species(R.sp[3 + j]);
+                    pb *= ipow3((double)c.C[s * kTile + tid] * cs, slot_nu(R.sp[3 + j]));
+                    g = fma(-(double)slot_nu(R.sp[3 + j]), c.G[s * kTile + tid], g);
+                }
+                if (R.flags & CG_F_REVERSIBLE) qb = kf * exp2(g) * pb;
+            } else {
+                const int gr = R.gen;
+                const int r0 = __ldg(m.gen_rptr + gr), r1 = __ldg(m.gen_rptr + gr + 1);
+                const int p0 = __ldg(m.gen_pptr + gr), p1 = __ldg(m.gen_pptr + gr + 1);
+                for (int j = r0; j < r1; ++j) {
+                    const int s = __ldg(m.gen_sp + j);
+                    const double nu = __ldg(m.gen_nu + j);
+                    qf *= pow((double)c.C[s * kTile + tid] * cs, nu);
+                    g = fma(nu, c.G[s * kTile + tid], g);
+                }
+                double pb = 1.0;
+                for (int j = p0; j < p1; ++j) {
+                    const int s = __ldg(m.gen_sp + j);
+                    const double nu = __ldg(m.gen_nu + j);
+                    pb *= pow((double)c.C[s * kTile + tid] * cs, nu);
+                    g = fma(-nu, c.G[s * kTile + tid], g);
+                }
+                if (R.flags & CG_F_REVERSIBLE) qb = kf * exp2(g) * pb;
+            }
+        }
+        double rr = qf - qb;
+        if (kind == CG_THIRD_BODY) rr *= (double)Ms * cs;
+        return (float)rr;
+    }
+    double a;
+    float sgn = 1.0f;
+    if (kind <= CG_THIRD_BODY) {
+        a = (fma(R.b, c.lnT, R.lnA) - R.theta * c.invT) * kLog2eD;
+        sgn = (float)R.sgn;
+    } else {
+        const DFall f = load_fall(m.fall + R.aux);
+        a = falloff_l2(kind, R.flags, R, f, __ldg(&m.fall2[R.aux].T2), Ms, c);
+    }
+    float cf = 1.0f;
+    int of = 0;
+    double g = 0.0;
+    for (int j = 0; j < R.nre; ++j) {
+        const int s = slot_species(R.sp[j]), nu = slot_nu(R.sp[j]);
+        const float x = c.C[s * kTile + tid];
+        cf *= (nu == 1) ? x : (nu == 2 ? x * x : x * x * x);
+        of += nu;
+        g = fma((double)nu, c.G[s * kTile + tid], g);
+    }
+    if (kind == CG_THIRD_BODY) {
+        cf *= Ms;
+        of += 1;
+    }
+    float q = rate32(a, cf, -32 * of);
+    if (R.flags & CG_F_REVERSIBLE) {
+        float cb = 1.0f;
+        int ob = 0;
+        for (int j = 0; j < R.npr; ++j) {
+            const int s = slot_species(R.sp[3 + j]), nu = slot_nu(R.sp[3 + j]);
+            const float x = c.C[s * kTile + tid];
+            cb *= (nu == 1) ? x : (nu == 2 ? x * x : x * x * x);
+            ob += nu;
+            g = fma(-(double)nu, c.G[s * kTile + tid], g);
+        }
+        if (kind == CG_THIRD_BODY) {
+            cb *= Ms;
+            ob += 1;
+        }
+        q -= rate32(a + g, cb, -32 * ob);
+    }
+    return sgn * q;
+}
+
+template <bool GS>
+__global__ void __launch_bounds__(kTile, 1)
+    getrates_tc_kernel(DevMech m, const __nv_bfloat16* __restrict__ nu, int npad, int nhalf, int nchunk, uint32_t tcols,
+                       const double* __restrict__ P, const double* __restrict__ Tg, const double* __restrict__ Y,
+                       double* __restrict__ wdot, int64_t ng, double* __restrict__ gscratch, int* err, int group) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ns = m.ns;
+    unsigned char* sA = sm;                                    // [2 buffers][3 splits][128 x 16] BF16
+    unsigned char* sB = sm + 6 * kABytes;                      // [2 buffers][npad x 16] BF16
+    float* sC = reinterpret_cast<float*>(sB + 2 * npad * 32);  // [ns][128]
+    double* sG = GS ? reinterpret_cast<double*>(sC + ns * kTile) : gscratch + (int64_t)blockIdx.x * ns * kTile;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(sC) + ns * kTile * 4 +
+                                                 (GS ? ns * kTile * 8 : 0));
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
+    if (tid == 0) {
+        um::mbar_init(&mbar[0], 1);
+        um::mbar_init(&mbar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) um::tmem_alloc(tslot, tcols);
+    um::fence_before_sync();
+    __syncthreads();
+    um::fence_after_sync();
+    const uint32_t tbase = *tslot;
+    uint32_t parity[2] = {0u, 0u};
+    bool pending[2] = {false, false};
+    bool ok = true;
+    const uint32_t idesc = um::idesc_bf16(kTile, nhalf);
+    const int nh = npad / nhalf;
+    const int64_t ntiles = (ng + kTile - 1) / kTile;
+    for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const int64_t i = tile * kTile + tid;
+        const bool act = i < ng;
+        TileCtx c;
+        c.C = sC;
+        c.G = sG;
+        c.T = act ? Tg[i] : 1000.0;
+        c.Pv = act ? P[i] : kPatm;
+        c.lnT = cgm::cg_log(c.T);
+        c.invT = 1.0 / c.T;
+        c.lnT2 = c.lnT * kLog2eD;
+        c.Tf = (float)c.T;
+        c.invTf = (float)c.invT;
+        c.lnT2f = (float)c.lnT2;
+        // Y -> C (ytoc.j2), stored as C * 2^32 in FP32
+        double csum = 0.0;
+        for (int k = 0; k < ns; ++k) {
+            const double yk = (act ? Y[(int64_t)k * ng + i] : 1.0) * __ldg(m.inv_mw + k);
+            sG[k * kTile + tid] = yk;
+            csum += yk;
+        }
+        const double facs = c.Pv / (kR0 * csum * c.T) * 4294967296.0;
+        double ctot = 0.0;
+        for (int k = 0; k < ns; ++k) {
+            const double cc = sG[k * kTile + tid] * facs;
+            sC[k * kTile + tid] = (float)cc;
+            ctot += cc;
+        }
+        c.ctot32 = (float)ctot;
+        // G = log2(exp(smh) Patm/(R0 T)) (exp_g.j2), FP64
+        const double lpfac2 = -6.35856916300311 - c.lnT2;   // log2(Patm/R0) - log2 T
+        for (int k = 0; k < ns; ++k)
+            sG[k * kTile + tid] = fma(species_smh(m.thermo, k, c.T, c.lnT, c.invT), kLog2eD, lpfac2);
+        bool first_group = true;
+        for (int ch = 0; ch < nchunk && ok; ++ch) {
+            const int buf = ch & 1;
+            if (pending[buf]) {
+                ok = um::mbar_wait(&mbar[buf], parity[buf]);
+                parity[buf] ^= 1u;
+                pending[buf] = false;
+                if (!ok) break;
+            }
+            // the chunk's stoichiometry, B operand [npad x 16], canonical layout
+            const uint4* src = reinterpret_cast<const uint4*>(nu + (int64_t)ch * npad * kChunk);
+            uint4* dst = reinterpret_cast<uint4*>(sB + buf * npad * 32);
+            for (int q = tid; q < npad * 2; q += kTile) dst[q] = __ldg(src + q);
+            // q for the chunk's reactions -> A operands (hi, mid, lo)
+            unsigned char* a0 = sA + buf * 3 * kABytes;
+            for (int j = 0; j < kChunk; ++j) {
+                const int r = ch * kChunk + j;
+                float q = (r < m.nr) ? rate_of_progress(m, r, c, tid) : 0.0f;
+                if (!act) q = 0.0f;
+                const __nv_bfloat16 h = __float2bfloat16_rn(q);
+                const float r1 = q - __bfloat162float(h);
+                const __nv_bfloat16 md = __float2bfloat16_rn(r1);
+                const __nv_bfloat16 lo = __float2bfloat16_rn(r1 - __bfloat162float(md));
+                const uint32_t off = um::kmajor_offset(tid, j, kChunk);
+                *reinterpret_cast<__nv_bfloat16*>(a0 + off) = h;
+                *reinterpret_cast<__nv_bfloat16*>(a0 + kABytes + off) = md;
+                *reinterpret_cast<__nv_bfloat16*>(a0 + 2 * kABytes + off) = lo;
+            }
+            um::fence_proxy_async();
+            um::fence_before_sync();
+            __syncthreads();
+            const bool group_start = (ch % group) == 0;
+            if (tid == 0) {
+                um::fence_after_sync();
+                const uint32_t bb = um::smem_addr(sB + buf * npad * 32);
+                for (int s = 0; s < 3; ++s) {
+                    const uint64_t ad = um::desc_kmajor(um::smem_addr(a0 + s * kABytes), kChunk, 0);
+                    for (int h = 0; h < nh; ++h)
+                        um::mma_bf16(tbase + (uint32_t)(h * nhalf), ad,
+                                     um::desc_kmajor(bb + (uint32_t)(h * nhalf * 32), kChunk, 0), idesc,
+                                     (!group_start || s > 0) ? 1u : 0u);
+                }
+                um::commit(&mbar[buf]);
+            }
+            pending[buf] = true;
+            if ((ch % group) == group - 1 || ch == nchunk - 1) {
+                // end of a group of reactions: wait for its MMAs, then add the
+                // FP32 partial sums into the FP64 output
+                for (int b = 0; b < 2; ++b)
+                    if (pending[b]) {
+                        ok = um::mbar_wait(&mbar[b], parity[b]) && ok;
+                        parity[b] ^= 1u;
+                        pending[b] = false;
+                    }
+                um::fence_after_sync();
+                if (ok) {
+                    for (int col = 0; col < npad; col += 16) {
+                        float v[16];
+                        um::tmem_ld16(um::tmem_lane_addr(tbase, warp, col), v);
+                        if (act)
+                            for (int j = 0; j < 16; ++j)
+                                if (col + j < ns) {
+                                    double* w = wdot + (int64_t)(col + j) * ng + i;
+                                    *w = first_group ? (double)v[j] : *w + (double)v[j];
+                                }
+                    }
+                }
+                first_group = false;
+                um::fence_before_sync();
+                __syncthreads();
+            }
+        }
+        um::fence_before_sync();
+        __syncthreads();
+    }
+    if (!ok && lane == 0) atomicExch(err, 1);
+    __syncthreads();
+    if (warp == 0) um::tmem_dealloc(tbase, tcols);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- host side
+cudaError_t mixed_prepare(const DevMech& m, const cg_mech_view& v, int device, MixedPlan** out) {
+    *out = nullptr;
+    const int ns = m.ns, nr = m.nr;
+    int npad = (ns + 31) / 32 * 32;
+    if (npad > 512) return cudaErrorNotSupported;     // TMEM holds 512 FP32 columns per lane
+    const int nhalf = npad <= 256 ? npad : npad / 2;
+    uint32_t tcols = 32;
+    while ((int)tcols < npad) tcols <<= 1;
+    const int nchunk = (nr + kChunk - 1) / kChunk;
+    const size_t base = 6 * (size_t)kABytes + 2 * (size_t)npad * 32 + (size_t)ns * kTile * 4 + 32;
+    const size_t with_g = base + (size_t)ns * kTile * 8;
+    cudaDeviceProp prop;
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return e;
+    const size_t limit = prop.sharedMemPerBlockOptin;
+    if (base > limit) return cudaErrorNotSupported;
+    MixedPlan* p = new MixedPlan();
+    p->ns = ns;
+    p->nr = nr;
+    p->npad = npad;
+    p->nhalf = nhalf;
+    p->nchunk = nchunk;
+    p->tcols = tcols;
+    p->g_smem = with_g <= limit ? 1 : 0;
+    // FP32 accumulation runs over `group` chunks (16 reactions each) before
+    // the partial sums are added into the FP64 output: 64 reactions for small
+    // mechanisms, 512 for large ones (where each flush moves ns doubles)
+    p->group = npad <= 128 ? 4 : 32;
+    p->smem = p->g_smem ? with_g : base;
+    // resident CTAs per SM, limited by shared memory and by 512 TMEM columns
+    int per_sm = (int)(prop.sharedMemPerMultiprocessor / (p->smem + 1024));
+    per_sm = std::min(per_sm, (int)(512 / tcols));
+    per_sm = std::max(per_sm, 1);
+    p->grid = prop.multiProcessorCount * per_sm;
+    // nu chunks in the canonical K-major layout: B[n][k] = nu of species n in reaction 16*chunk + k
+    std::vector<float> nuf((size_t)ns * nr, 0.0f);
+    const int32_t* rp = (const int32_t*)v.a[CG_RPTR];
+    const int32_t* pp = (const int32_t*)v.a[CG_PPTR];
+    const int32_t* rsp = (const int32_t*)v.a[CG_RSP];
+    const int32_t* psp = (const int32_t*)v.a[CG_PSP];
+    const double* rnu = (const double*)v.a[CG_RNU];
+    const double* pnu = (const double*)v.a[CG_PNU];
+    for (int r = 0; r < nr; ++r) {
+        for (int j = rp[r]; j < rp[r + 1]; ++j) nuf[(size_t)rsp[j] * nr + r] -= (float)rnu[j];
+        for (int j = pp[r]; j < pp[r + 1]; ++j) nuf[(size_t)psp[j] * nr + r] += (float)pnu[j];
+    }
+    std::vector<__nv_bfloat16> img((size_t)nchunk * npad * kChunk, __float2bfloat16(0.0f));
+    bool exact = true;
+    for (int ch = 0; ch < nchunk; ++ch)
+        for (int n = 0; n < ns; ++n)
+            for (int k = 0; k < kChunk; ++k) {
+                const int r = ch * kChunk + k;
+                if (r >= nr) continue;
+                const float x = nuf[(size_t)n * nr + r];
+                const __nv_bfloat16 b = __float2bfloat16(x);
+                if (__bfloat162float(b) != x) exact = false;
+                const size_t off = ((size_t)(n >> 3) * (kChunk * 16) + (k >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2) / 2;
+                img[(size_t)ch * npad * kChunk + off] = b;
+            }
+    if (!exact) {
+        delete p;
+        return cudaErrorNotSupported;                  // coefficients not exact in BF16
+    }
+    const size_t bytes = img.size() * sizeof(__nv_bfloat16) + 256;
+    e = cudaMalloc(&p->dbuf, bytes);
+    if (e == cudaSuccess) e = cudaMemcpy(p->dbuf, img.data(), img.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset((char*)p->dbuf + bytes - 256, 0, 256);
+    if (e == cudaSuccess) {
+        auto k64 = getrates_tc_kernel<true>;
+        auto k32 = getrates_tc_kernel<false>;
+        e = cudaFuncSetAttribute(p->g_smem ? k64 : k32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem);
+    }
+    if (e != cudaSuccess) {
+        if (p->dbuf) cudaFree(p->dbuf);
+        delete p;
+        return e;
+    }
+    p->nu = (const __nv_bfloat16*)p->dbuf;
+    p->err = (int*)((char*)p->dbuf + bytes - 256);
+    *out = p;
+    return cudaSuccess;
+}
+
+void mixed_release(MixedPlan* p) {
+    if (!p) return;
+    if (p->dbuf) cudaFree(p->dbuf);
+    delete p;
+}
+
+size_t mixed_workspace_bytes(const MixedPlan* p, int64_t ng) {
+    if (!p || p->g_smem) return 0;
+    int64_t tiles = (ng + kTile - 1) / kTile;
+    int64_t grid = std::min<int64_t>(tiles, p->grid);
+    return (size_t)grid * p->ns * kTile * sizeof(double);
+}
+
+cudaError_t launch_getrates_mixed(const MixedPlan* p, const DevMech& m, const double* P, const double* T,
+                                  const double* Y, double* wdot, int64_t ng, void* scratch, size_t scratch_bytes,
+                                  cudaStream_t s) {
+    if (ng <= 0) return cudaSuccess;
+    int64_t tiles = (ng + kTile - 1) / kTile;
+    int64_t grid = std::min<int64_t>(tiles, p->grid);
+    if (!p->g_smem) {
+        const int64_t fit = (int64_t)(scratch_bytes / ((size_t)p->ns * kTile * sizeof(double)));
+        grid = std::min<int64_t>(grid, fit);
+        if (grid < 1 || !scratch) return cudaErrorInvalidValue;
+    }
+    if (p->g_smem)
+        getrates_tc_kernel<true><<<(unsigned)grid, kTile, p->smem, s>>>(m, p->nu, p->npad, p->nhalf, p->nchunk, p->tcols,
+                                                                        P, T, Y, wdot, ng, nullptr, p->err, p->group);
+    else
+        getrates_tc_kernel<false><<<(unsigned)grid, kTile, p->smem, s>>>(m, p->nu, p->npad, p->nhalf, p->nchunk,
+                                                                         p->tcols, P, T, Y, wdot, ng, (double*)scratch,
+                                                                         p->err, p->group);
+    return cudaGetLastError();
+}
+
+int mixed_error_flag(const MixedPlan* p) {
+    int v = 0;
+    if (!p || cudaMemcpy(&v, p->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    return v;
+}
+
+}  // namespace cg

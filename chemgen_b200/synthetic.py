@@ -12,8 +12,10 @@ and are identical on every machine.  Rules:
 * every reaction is oriented exothermic in the forward direction, so the
   reverse rate kf/Kc carries an activation energy of Ea + |dH| (a random
   endothermic reaction with Ea = 0 would produce reverse rates no real
-  mechanism has), and reactions with max |d(g/RT)| > 300 over 300..2500 K are
-  redrawn (real mechanisms reach about 314);
+  mechanism has); reactions with max |d(g/RT)| > 300 over 300..2500 K (real
+  mechanisms reach about 314) or with ln Kc < -20 anywhere in that range
+  (a reverse rate above e^20 kf, which random entropy differences can
+  produce) are redrawn;
 * states: T ~ U(300, 2500) K, P = 1 atm * exp(U(0, ln 40)) in dyne/cm^2,
   Y ~ Dirichlet(0.5), float64, species-major (``Y[k, i]``).
 """
@@ -120,6 +122,12 @@ def synthetic_mechanism(ns: int, nr: int, n_third_body: int, n_troe: int, seed: 
                 - sum(n * _hrt(species[names.index(s)], 1000.0) for s, n in reac.items())
             if dh > 0.0:
                 reac, prod = prod, reac
+                d = -d
+            # ln Kc (concentration units) = d(smh) + dnu ln(Patm/(R0 T))
+            dnu = sum(prod.values()) - sum(reac.values())
+            lnkc = d + dnu * np.log(PATM / (8.314510e07 * Tgrid))
+            if lnkc.min() < -20.0:
+                continue
             break
         rev = bool(rng.random() < frac_reversible)
         arh = _arrhenius(rng)
