@@ -67,6 +67,20 @@ def lib() -> ctypes.CDLL:
     L.chemgen_getrates_vjp.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp, vp, vp]
     L.chemgen_getrates_noalloc.argtypes = [vp, vp, vp, i64, vp, vp, vp]
     L.chemgen_getrates_noalloc.restype = ci
+    f32 = ctypes.c_float
+    L.chemgen_mlp_gemm.argtypes = [vp, i64, i64, vp, i64, i64, vp, i64, ci, ci, ci, ci, vp]
+    L.chemgen_mlp_bias_gelu.argtypes = [vp, vp, vp, i64, ci, ci, vp]
+    L.chemgen_mlp_gelu_backward.argtypes = [vp, vp, vp, vp, i64, vp]
+    L.chemgen_mlp_mse_grad.argtypes = [vp, vp, vp, vp, vp, vp, i64, ci, vp]
+    L.chemgen_mlp_colsum.argtypes = [vp, vp, i64, ci, vp]
+    L.chemgen_mlp_adam.argtypes = [vp, vp, vp, vp, vp, i64, vp, f32, f32, f32, f32, vp]
+    L.chemgen_surrogate_features.argtypes = [vp, vp, vp, i64, ci, ci, vp, vp, vp, vp, vp]
+    L.chemgen_surrogate_targets.argtypes = [vp, i64, ci, ci, vp, vp, vp]
+    L.chemgen_surrogate_decode.argtypes = [vp, i64, ci, ci, vp, vp, vp, vp]
+    for f in ("chemgen_mlp_gemm", "chemgen_mlp_bias_gelu", "chemgen_mlp_gelu_backward", "chemgen_mlp_mse_grad",
+              "chemgen_mlp_colsum", "chemgen_mlp_adam", "chemgen_surrogate_features", "chemgen_surrogate_targets",
+              "chemgen_surrogate_decode"):
+        getattr(L, f).restype = ci
     L.chemgen_use_generated.argtypes = [vp, ci]
     L.chemgen_kernel_kind.argtypes = [vp, ci]
     L.chemgen_register_kernels.argtypes = [ctypes.c_uint64, ci, ci, ctypes.c_uint, vp]

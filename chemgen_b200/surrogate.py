@@ -1,0 +1,475 @@
+"""Learned surrogate of getrates with per-point fallback to the exact kernel.
+
+Network: inputs (1000/T, ln T, ln P and the ln mole fraction of each of the
+ns species, centred and scaled) padded to `din`, each held as a BF16 pair
+(hi + lo) that the first layer multiplies by the same weights; three hidden
+layers of width 256 with GELU; `dout` outputs: the direction
+u_k = w_k / |w|_2 of the rate vector (columns 0..ns-1), its centred log
+length (ln |w|_2 - c) / s (column ns) and an estimate of log10 of the
+network's own normwise error at that point (column ns + 1).  Because the
+normwise error of a decoded prediction is, to first order,
+max_k |du_k| / max_k |u_k| + |d ln |w|_2|, the regression loss weighs the
+outputs the way the error gate judges them.  BF16 weights (FP32 master
+copies) and FP32 accumulation.
+
+Training runs entirely on this package's CUDA kernels (chemgen_mlp_* in
+libchemgen_b200.so): the forward products, the input and weight gradients,
+GELU and its derivative, the loss gradient, bias sums and Adam; one training
+step is captured as a CUDA graph and replayed.  The training data are
+(P, T, Y) -> wdot samples produced by the exact kernel.
+
+Inference (`SurrogateGetrates`): the network predicts wdot and its error
+estimate; a point falls back to the exact kernel when its inputs leave the
+training ranges or the estimate exceeds the tolerance.  The exact kernel is
+also the judge used to report the surrogate's accuracy.
+
+The reference has no surrogate; its chemgen/chemistry_nn.py:15-85 torch
+prototype (log-space Arrhenius layers) never ran.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass
+from typing import Dict, List
+
+from .runtime import GpuMechanism, check, lib
+
+HIDDEN = 256
+DIN = 64
+DOUT = 64
+
+
+def _stream():
+    import torch
+    return torch.cuda.current_stream().cuda_stream
+
+
+@dataclass
+class TrainConfig:
+    samples: int = 10_000_000
+    batch: int = 1024
+    epochs: int = 16
+    lr: float = 1e-3
+    lr_final: float = 5e-5
+    weight_decay: float = 0.0
+    error_head_epochs: int = 1
+    seed: int = 0
+
+
+class MLP:
+    """The network's parameters and the kernel calls of one forward/backward."""
+
+    def __init__(self, din: int = DIN, hidden: int = HIDDEN, dout: int = DOUT, seed: int = 0, device: int = 0):
+        import torch
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        self.dims = [din, hidden, hidden, hidden, dout]
+        self.dev = torch.device("cuda", device)
+        self.W: List = []       # FP32 master [N x K]
+        self.Wb: List = []      # BF16 copy
+        self.b: List = []
+        for l in range(4):
+            k, n = self.dims[l], self.dims[l + 1]
+            w = torch.randn(n, k, generator=g) * math.sqrt(2.0 / k)
+            self.W.append(w.to(self.dev).contiguous())
+            self.Wb.append(self.W[-1].to(torch.bfloat16).contiguous())
+            self.b.append(torch.zeros(n, device=self.dev))
+        self.params = self.W + self.b
+        self.m = [torch.zeros_like(p) for p in self.params]
+        self.v = [torch.zeros_like(p) for p in self.params]
+        self._ws: Dict = {}
+
+    def _buf(self, key, shape, dtype):
+        import torch
+        t = self._ws.get(key)
+        if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype:
+            t = torch.empty(shape, dtype=dtype, device=self.dev)
+            self._ws[key] = t
+        return t
+
+    def _input_parts(self, X):
+        """(pointer, row stride) of each BF16 part of the input: one part for
+        X [B, din], two (hi, lo) for X [B, 2 din], whose sum is the input."""
+        din = self.dims[0]
+        if X.shape[1] == din:
+            return [(X.data_ptr(), din)]
+        if X.shape[1] == 2 * din:
+            return [(X.data_ptr(), 2 * din), (X.data_ptr() + 2 * din, 2 * din)]
+        raise ValueError(f"input width {X.shape[1]} is neither {din} nor {2 * din}")
+
+    def forward(self, X, keep: bool = True):
+        """X: BF16 [B, din], or [B, 2 din] holding hi and lo parts.  Returns
+        the FP32 output [B, dout]; keeps Z_l and H_l for the backward when
+        `keep`."""
+        import torch
+        B = X.shape[0]
+        s = _stream()
+        H = X
+        self.acts = [X]
+        self.zs = []
+        for l in range(4):
+            k, n = self.dims[l], self.dims[l + 1]
+            Z = self._buf(("Z", l, keep), (B, n), torch.float32)
+            parts = self._input_parts(X) if l == 0 else [(H.data_ptr(), k)]
+            for j, (ptr, ld) in enumerate(parts):
+                check(lib().chemgen_mlp_gemm(ptr, ld, 1, self.Wb[l].data_ptr(), k, 1, Z.data_ptr(), n, B, n, k,
+                                             1 if j else 0, s), "mlp_gemm")
+            Hn = self._buf(("H", l, keep), (B, n), torch.bfloat16) if l < 3 else None
+            check(lib().chemgen_mlp_bias_gelu(Z.data_ptr(), self.b[l].data_ptr(), 0 if Hn is None else Hn.data_ptr(),
+                                              B, n, 1 if l < 3 else 0, s), "mlp_bias_gelu")
+            self.zs.append(Z)
+            if Hn is not None:
+                self.acts.append(Hn)
+                H = Hn
+        return self.zs[-1]
+
+    def backward(self, dout_b, dout_f):
+        """dout: gradient of the loss wrt the output (BF16 and FP32 [B, dout]).
+        Returns the parameter gradients (same order as self.params)."""
+        import torch
+        B = dout_b.shape[0]
+        s = _stream()
+        gW = [None] * 4
+        gb = [None] * 4
+        dZb, dZf = dout_b, dout_f
+        for l in range(3, -1, -1):
+            k, n = self.dims[l], self.dims[l + 1]
+            H = self.acts[l]
+            gw = self._buf(("gW", l), (n, k), torch.float32)
+            # gW[n][k] = sum_m dZ[m][n] H[m][k]
+            parts = self._input_parts(H) if l == 0 else [(H.data_ptr(), k)]
+            for j, (ptr, ld) in enumerate(parts):
+                check(lib().chemgen_mlp_gemm(dZb.data_ptr(), 1, n, ptr, 1, ld, gw.data_ptr(), k, n, k, B, 1 if j else 0,
+                                             s), "mlp_gemm dW")
+            g_b = self._buf(("gb", l), (n,), torch.float32)
+            check(lib().chemgen_mlp_colsum(dZf.data_ptr(), g_b.data_ptr(), B, n, s), "mlp_colsum")
+            gW[l], gb[l] = gw, g_b
+            if l == 0:
+                break
+            # dH[m][k] = sum_n dZ[m][n] W[n][k]
+            dH = self._buf(("dH", l), (B, k), torch.float32)
+            check(lib().chemgen_mlp_gemm(dZb.data_ptr(), n, 1, self.Wb[l].data_ptr(), 1, k, dH.data_ptr(), k, B, k, n,
+                                         0, s), "mlp_gemm dH")
+            nb = self._buf(("dZb", l - 1), (B, k), torch.bfloat16)
+            nf = self._buf(("dZf", l - 1), (B, k), torch.float32)
+            check(lib().chemgen_mlp_gelu_backward(dH.data_ptr(), self.zs[l - 1].data_ptr(), nb.data_ptr(),
+                                                  nf.data_ptr(), B * k, s), "mlp_gelu_backward")
+            dZb, dZf = nb, nf
+        return gW + gb
+
+    def adam(self, grads, hyper, wd: float = 0.0, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8):
+        """One Adam step; `hyper` is a device FP32 tensor {lr, 1/(1-b1^t), 1/(1-b2^t)}."""
+        s = _stream()
+        for j, (p, g) in enumerate(zip(self.params, grads)):
+            wb = self.Wb[j].data_ptr() if j < 4 else 0
+            check(lib().chemgen_mlp_adam(p.data_ptr(), g.data_ptr(), self.m[j].data_ptr(), self.v[j].data_ptr(), wb,
+                                         p.numel(), hyper.data_ptr(), b1, b2, eps, wd if j < 4 else 0.0, s),
+                  "mlp_adam")
+
+
+def adam_schedule(total: int, lr: float, lr_final: float, b1: float = 0.9, b2: float = 0.999, device=None):
+    """[total, 3] FP32 rows {lr_t, 1/(1-b1^t), 1/(1-b2^t)} for t = 1..total,
+    lr_t on a cosine from lr to lr_final."""
+    import torch
+    t = torch.arange(1, total + 1, dtype=torch.float64)
+    frac = (t - 1) / max(total - 1, 1)
+    lrs = lr_final + 0.5 * (lr - lr_final) * (1.0 + torch.cos(math.pi * frac))
+    return torch.stack([lrs, 1.0 / (1.0 - b1 ** t), 1.0 / (1.0 - b2 ** t)], dim=1).float().to(device)
+
+
+class Surrogate:
+    """MLP surrogate for one mechanism, trained from the exact kernel."""
+
+    def __init__(self, gm: GpuMechanism, seed: int = 0, device: int = 0):
+        import torch
+        if gm.ns + 2 > DOUT or gm.ns + 3 > DIN:
+            raise ValueError(f"the surrogate supports up to {DOUT - 2} species")
+        if gm.mech is None:
+            raise ValueError("the surrogate needs the mechanism's molecular weights (construct GpuMechanism from a "
+                             "Mechanism)")
+        self.gm = gm
+        self.ns = gm.ns
+        self.net = MLP(seed=seed, device=device)
+        self.dev = self.net.dev
+        self.inv_mw = 1.0 / torch.tensor(gm.mech.mw(), dtype=torch.float64, device=self.dev)
+        # centring and scaling of 1000/T, ln T and ln(P/1 atm) over the
+        # training ranges (T 300..2500 K, P 1..40 atm); those of ln X_k are
+        # set from the training data in fit()
+        self.norm = torch.tensor([1.3, 1.0 / 0.9, 6.9, 1.0 / 0.55, math.log(40.0) / 2,
+                                  1.0 / (math.log(40.0) / math.sqrt(12.0)), 0.0, 1.0], device=self.dev)
+        self.lnorm = torch.tensor([0.0, 1.0], device=self.dev)
+        self.colw = torch.zeros(DOUT, device=self.dev)
+        self.T_range = (300.0, 2500.0)
+        self.P_range = (1013250.0, 1013250.0 * 40.0)
+        self.history: List[float] = []
+
+    # ------------------------------------------------------------ transforms
+    def features(self, P, T, Y):
+        """BF16 [ng, 2 din]: the hi and lo parts of the network inputs."""
+        import torch
+        ng = T.numel()
+        X = torch.empty((ng, 2 * DIN), dtype=torch.bfloat16, device=self.dev)
+        check(lib().chemgen_surrogate_features(P.data_ptr(), T.data_ptr(), Y.data_ptr(), ng, self.ns, DIN,
+                                               self.norm.data_ptr(), self.inv_mw.data_ptr(), X.data_ptr(), 0,
+                                               _stream()), "features")
+        return X
+
+    def targets(self, W):
+        import torch
+        ng = W.shape[1]
+        Tg = torch.empty((ng, DOUT), dtype=torch.float32, device=self.dev)
+        check(lib().chemgen_surrogate_targets(W.data_ptr(), ng, self.ns, DOUT, self.lnorm.data_ptr(), Tg.data_ptr(),
+                                              _stream()), "targets")
+        return Tg
+
+    def decode(self, out):
+        import torch
+        ng = out.shape[0]
+        W = torch.empty((self.ns, ng), dtype=torch.float64, device=self.dev)
+        est = torch.empty(ng, dtype=torch.float32, device=self.dev)
+        check(lib().chemgen_surrogate_decode(out.data_ptr(), ng, self.ns, DOUT, self.lnorm.data_ptr(), W.data_ptr(),
+                                             est.data_ptr(), _stream()), "decode")
+        return W, est
+
+    def _set_species_norm(self, Y):
+        """Centre and spread of ln X_k over a sample of states."""
+        import torch
+        n = Y.clamp_min(1e-30) * self.inv_mw[:, None]
+        lx = torch.log(n) - torch.log(n.sum(dim=0, keepdim=True))
+        self.norm[6] = float(lx.mean())
+        self.norm[7] = 1.0 / float(lx.std())
+
+    # --------------------------------------------------------------- data
+    def sample_states(self, n: int, gen):
+        """States with the workload's distributions (T ~ U(300, 2500) K, P
+        log-uniform over 1..40 atm, Y ~ Dirichlet(0.5)), drawn on the GPU."""
+        import torch
+        T = torch.rand(n, generator=gen, device=self.dev, dtype=torch.float64) * 2200.0 + 300.0
+        P = 1013250.0 * torch.exp(torch.rand(n, generator=gen, device=self.dev, dtype=torch.float64) * math.log(40.0))
+        G = torch._standard_gamma(torch.full((self.ns, n), 0.5, device=self.dev, dtype=torch.float64), generator=gen)
+        Y = (G / G.sum(dim=0, keepdim=True)).contiguous()
+        return P.contiguous(), T.contiguous(), Y
+
+    def make_dataset(self, n: int, seed: int, chunk: int = 1 << 20, mode: str = "fp64"):
+        """(features BF16 [n, 2 din] chunks, wdot FP64 [ns, n] chunks) from the exact kernel."""
+        import torch
+        gen = torch.Generator(device=self.dev).manual_seed(seed)
+        Xs, Ws = [], []
+        for i0 in range(0, n, chunk):
+            m = min(chunk, n - i0)
+            P, T, Y = self.sample_states(m, gen)
+            if i0 == 0:
+                self._set_species_norm(Y)
+            W = self.gm.getrates(P, T, Y, mode=mode)
+            Xs.append(self.features(P, T, Y))
+            Ws.append(W)
+        return Xs, Ws
+
+    # ------------------------------------------------------------- training
+    def fit(self, cfg: TrainConfig = TrainConfig(), log=None, graph: bool = True) -> Dict:
+        """Train on cfg.samples exact-kernel samples.  The training step (batch
+        gather, forward, loss gradient, backward, Adam) is captured once as a
+        CUDA graph and replayed; per step only the batch indices and the
+        schedule row are copied in."""
+        import torch
+        t0 = time.perf_counter()
+        Xs, Ws = self.make_dataset(cfg.samples, cfg.seed)
+        # centre and spread of ln |w|_2 over the first chunk; the log-length
+        # column is weighted by spread^2 so that its loss is in units of ln |w|_2
+        ln_n = torch.log(Ws[0].norm(dim=0).clamp_min(1e-300))
+        self.lnorm[0] = float(ln_n.mean())
+        self.lnorm[1] = float(ln_n.std().clamp_min(1e-3))
+        self.colw.zero_()
+        self.colw[: self.ns] = 1.0
+        self.colw[self.ns] = float(self.lnorm[1]) ** 2
+        X = torch.cat(Xs)
+        Tg = torch.cat([self.targets(W) for W in Ws])
+        del Xs, Ws
+        n = X.shape[0]
+        torch.cuda.synchronize(self.dev)
+        t_data = time.perf_counter() - t0
+        B = cfg.batch
+        steps_per_epoch = n // B
+        total = steps_per_epoch * cfg.epochs
+        sched = adam_schedule(total, cfg.lr, cfg.lr_final, device=self.dev)
+        hyper = torch.empty(3, device=self.dev)
+        idx = torch.zeros(B, dtype=torch.int64, device=self.dev)
+        xb = torch.empty((B, X.shape[1]), dtype=X.dtype, device=self.dev)
+        tb = torch.empty((B, DOUT), dtype=torch.float32, device=self.dev)
+        loss = torch.zeros(1, device=self.dev)
+        dout_b = torch.empty((B, DOUT), dtype=torch.bfloat16, device=self.dev)
+        dout_f = torch.empty((B, DOUT), dtype=torch.float32, device=self.dev)
+        gen = torch.Generator(device=self.dev).manual_seed(cfg.seed + 1)
+
+        def body():
+            torch.index_select(X, 0, idx, out=xb)
+            torch.index_select(Tg, 0, idx, out=tb)
+            out = self.net.forward(xb)
+            check(lib().chemgen_mlp_mse_grad(out.data_ptr(), tb.data_ptr(), self.colw.data_ptr(), dout_b.data_ptr(),
+                                             dout_f.data_ptr(), loss.data_ptr(), B, DOUT, _stream()), "mse_grad")
+            grads = self.net.backward(dout_b, dout_f)
+            self.net.adam(grads, hyper, cfg.weight_decay)
+
+        g = None
+        step = 0
+        t1 = time.perf_counter()
+        for ep in range(cfg.epochs):
+            perm = torch.randperm(n, device=self.dev, generator=gen)
+            loss.zero_()
+            for b in range(steps_per_epoch):
+                idx.copy_(perm[b * B:(b + 1) * B])
+                hyper.copy_(sched[step])
+                if g is not None:
+                    g.replay()
+                else:
+                    body()
+                    if graph and step == 2:
+                        # capture after a few eager steps, once every buffer exists
+                        torch.cuda.synchronize(self.dev)
+                        side = torch.cuda.Stream(device=self.dev)
+                        side.wait_stream(torch.cuda.current_stream())
+                        g = torch.cuda.CUDAGraph()
+                        with torch.cuda.stream(side):
+                            with torch.cuda.graph(g, stream=side):
+                                body()
+                        torch.cuda.current_stream().wait_stream(side)
+                step += 1
+            self.history.append(loss.item() / max(steps_per_epoch, 1))
+            if log:
+                log(f"epoch {ep}: loss {self.history[-1]:.4e}")
+        torch.cuda.synchronize(self.dev)
+        t_train = time.perf_counter() - t1
+        del g
+        # error head: regress log10 of the per-point normwise error of the
+        # decoded prediction, on the same data, with the same kernels
+        t2 = time.perf_counter()
+        self.fit_error_head(X, Tg, cfg, gen, log)
+        torch.cuda.synchronize(self.dev)
+        t_head = time.perf_counter() - t2
+        return {"samples": n, "t_data_s": t_data, "t_train_s": t_train, "t_error_head_s": t_head,
+                "steps": step, "final_loss": self.history[-1] if self.history else None}
+
+    def _normwise_error(self, out, tgt):
+        """log10 of max_k |w_hat - w| / max_k |w| per row, from network-space
+        tensors (both vectors divided by the true |w|_2)."""
+        import torch
+        ns = self.ns
+        r = torch.exp(((out[:, ns] - tgt[:, ns]) * self.lnorm[1]).clamp(-30.0, 30.0))
+        e = (out[:, :ns] * r[:, None] - tgt[:, :ns]).abs().max(dim=1).values
+        e = e / tgt[:, :ns].abs().max(dim=1).values.clamp_min(1e-30)
+        return torch.log10(e.clamp_min(1e-12))
+
+    def fit_error_head(self, X, Tg, cfg: TrainConfig, gen, log=None):
+        import torch
+        n = X.shape[0]
+        colw = torch.zeros(DOUT, device=self.dev)
+        colw[self.ns + 1] = 1.0
+        loss = torch.zeros(1, device=self.dev)
+        dout_b = torch.empty((cfg.batch, DOUT), dtype=torch.bfloat16, device=self.dev)
+        dout_f = torch.empty((cfg.batch, DOUT), dtype=torch.float32, device=self.dev)
+        s = _stream()
+        per_epoch = max(n // cfg.batch, 1)
+        steps = per_epoch * cfg.error_head_epochs
+        perm = torch.randperm(n, device=self.dev, generator=gen)
+        hm = [torch.zeros_like(self.net.W[3]), torch.zeros_like(self.net.b[3])]
+        hv = [torch.zeros_like(self.net.W[3]), torch.zeros_like(self.net.b[3])]
+        keep = torch.zeros(DOUT, device=self.dev)
+        keep[self.ns + 1] = 1.0
+        sched = adam_schedule(max(steps, 1), 1e-3, 1e-3, device=self.dev)
+        for b in range(steps):
+            j = b % per_epoch
+            idx = perm[j * cfg.batch:(j + 1) * cfg.batch]
+            xb = X.index_select(0, idx)
+            tb = Tg.index_select(0, idx)
+            out = self.net.forward(xb)
+            tb[:, self.ns + 1] = self._normwise_error(out, tb)
+            check(lib().chemgen_mlp_mse_grad(out.data_ptr(), tb.data_ptr(), colw.data_ptr(), dout_b.data_ptr(),
+                                             dout_f.data_ptr(), loss.data_ptr(), xb.shape[0], DOUT, s), "mse_grad")
+            grads = self.net.backward(dout_b[: xb.shape[0]], dout_f[: xb.shape[0]])
+            # only the error-estimate output (row ns + 1 of the last layer and
+            # its bias) moves, with its own Adam state
+            gW4, gb4 = grads[3], grads[7]
+            gW4.mul_(keep[:, None])
+            gb4.mul_(keep)
+            hyper = sched[b]
+            for p, g, m, v, wb in ((self.net.W[3], gW4, hm[0], hv[0], self.net.Wb[3]),
+                                   (self.net.b[3], gb4, hm[1], hv[1], None)):
+                check(lib().chemgen_mlp_adam(p.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(),
+                                             0 if wb is None else wb.data_ptr(), p.numel(), hyper.data_ptr(), 0.9,
+                                             0.999, 1e-8, 0.0, s), "mlp_adam")
+        if log:
+            log(f"error head: loss {loss.item() / max(steps, 1):.4e}")
+
+    # ------------------------------------------------------------ checkpoint
+    def _mech_hash(self) -> str:
+        import hashlib
+        return hashlib.sha256(bytes(self.gm.blob)).hexdigest()
+
+    def state_dict(self) -> Dict:
+        """Weights (FP32 masters), biases and the input/output normalisation."""
+        return {"W": [w.cpu() for w in self.net.W], "b": [b.cpu() for b in self.net.b], "norm": self.norm.cpu(),
+                "lnorm": self.lnorm.cpu(), "ns": self.ns, "mechanism_sha256": self._mech_hash()}
+
+    def load_state_dict(self, st: Dict) -> None:
+        import torch
+        if st["ns"] != self.ns or st.get("mechanism_sha256") != self._mech_hash():
+            raise ValueError("the checkpoint was trained on a different mechanism")
+        for l in range(4):
+            self.net.W[l].copy_(st["W"][l].to(self.dev))
+            self.net.Wb[l].copy_(self.net.W[l].to(torch.bfloat16))
+            self.net.b[l].copy_(st["b"][l].to(self.dev))
+        self.norm.copy_(st["norm"].to(self.dev))
+        self.lnorm.copy_(st["lnorm"].to(self.dev))
+
+    def save(self, path: str) -> None:
+        import torch
+        torch.save(self.state_dict(), path)
+
+    def load(self, path: str) -> None:
+        import torch
+        self.load_state_dict(torch.load(path, map_location="cpu"))
+
+    # ------------------------------------------------------------- inference
+    def predict(self, P, T, Y, chunk: int = 1 << 20):
+        """(wdot [ns, ng] FP64, log10 error estimate [ng])."""
+        import torch
+        ng = T.numel()
+        W = torch.empty((self.ns, ng), dtype=torch.float64, device=self.dev)
+        est = torch.empty(ng, dtype=torch.float32, device=self.dev)
+        for i0 in range(0, ng, chunk):
+            i1 = min(ng, i0 + chunk)
+            X = self.features(P[i0:i1].contiguous(), T[i0:i1].contiguous(), Y[:, i0:i1].contiguous())
+            out = self.net.forward(X, keep=False)
+            w, e = self.decode(out)
+            W[:, i0:i1] = w
+            est[i0:i1] = e
+        return W, est
+
+    def in_range(self, P, T, Y):
+        """Points inside the training distribution's support."""
+        ok = (T >= self.T_range[0]) & (T <= self.T_range[1]) & (P >= self.P_range[0] * 0.999) & \
+             (P <= self.P_range[1] * 1.001)
+        ok &= (Y >= 0).all(dim=0) & ((Y.sum(dim=0) - 1.0).abs() < 1e-6)
+        return ok
+
+
+class SurrogateGetrates:
+    """wdot from the surrogate where it is trusted, from the exact kernel elsewhere."""
+
+    def __init__(self, sur: Surrogate, tol: float, exact_mode: str = "mixed"):
+        self.sur = sur
+        self.tol = tol
+        self.exact_mode = exact_mode
+        self.last_fallback = 0.0
+
+    def __call__(self, P, T, Y):
+        import torch
+        W, est = self.sur.predict(P, T, Y)
+        ok = self.sur.in_range(P, T, Y) & (est <= math.log10(self.tol))
+        bad = torch.nonzero(~ok).flatten()
+        if bad.numel():
+            Pb, Tb = P.index_select(0, bad).contiguous(), T.index_select(0, bad).contiguous()
+            Yb = Y.index_select(1, bad).contiguous()
+            W[:, bad] = self.sur.gm.getrates(Pb, Tb, Yb, mode=self.exact_mode)
+        self.last_fallback = bad.numel() / max(T.numel(), 1)
+        return W

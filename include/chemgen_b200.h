@@ -113,6 +113,41 @@ int chemgen_jacobian(chemgen_handle* h, int precision, const double* P, const do
 int chemgen_getrates_vjp(chemgen_handle* h, const double* P, const double* T, int64_t ng, const double* Y,
                          const double* G, double* gT, double* gY, double* gP, void* stream);
 
+/* Learned surrogate of wdot (no counterpart in the reference; its torch
+ * prototype chemgen/chemistry_nn.py:15-85 never ran).  Building blocks of a
+ * BF16 MLP (FP32 accumulation) trained and evaluated on the GPU; all pointers
+ * are device pointers, all calls asynchronous on `stream`.
+ * chemgen_mlp_gemm: C[i*ldc + j] (+)= sum_r A[i*sai + r*sar] * B[j*sbj + r*sbr]
+ *   for i < M, j < N, r < R (A, B BF16; C FP32; accumulate != 0 adds).
+ * chemgen_mlp_bias_gelu: Z += bias (per column); H = GELU(Z) (tanh form) or Z, BF16.
+ * chemgen_mlp_gelu_backward: dZ = dH * GELU'(Z) (BF16, and FP32 if dZf).
+ * chemgen_mlp_mse_grad: loss += mean_rows sum_j colw_j (out - target)^2, dout = its gradient.
+ * chemgen_mlp_colsum: db[n] = sum_m dZ[m*N + n].
+ * chemgen_mlp_adam: Adam step (weight decay wd) on FP32 w, BF16 copy to wb (if non-NULL); the
+ *   learning rate and bias corrections are read on the device from hyper = {lr, 1/(1-b1^t), 1/(1-b2^t)}.
+ * chemgen_surrogate_features: per point the din values (1000/T, ln T, ln(P/1 atm), ln X_k for the
+ *   ns species (mole fractions from Y and inv_mw; ln Y_k when inv_mw is NULL), zeros), each centred
+ *   and scaled by the pairs in norm[0..7] (species values clipped to [-6, 6]); stored as BF16 hi
+ *   parts in X[i*2*din + j] and BF16 remainders in X[i*2*din + din + j] (+FP32 in Xf if non-NULL).
+ * chemgen_surrogate_targets: T[i*dout + k] = w_k / |w|_2 for k < ns, (ln |w|_2 - lnorm[0]) / lnorm[1]
+ *   for k = ns, 0 beyond.
+ * chemgen_surrogate_decode: the inverse, W[k*ng + i]; err_est[i] = column ns + 1. */
+int chemgen_mlp_gemm(const void* A, int64_t sai, int64_t sar, const void* B, int64_t sbj, int64_t sbr, float* C,
+                     int64_t ldc, int M, int N, int R, int accumulate, void* stream);
+int chemgen_mlp_bias_gelu(float* Z, const float* bias, void* H, int64_t M, int N, int apply_gelu, void* stream);
+int chemgen_mlp_gelu_backward(const float* dH, const float* Z, void* dZ, float* dZf, int64_t n, void* stream);
+int chemgen_mlp_mse_grad(const float* out, const float* target, const float* colw, void* dout, float* doutf,
+                         float* loss, int64_t M, int N, void* stream);
+int chemgen_mlp_colsum(const float* dZ, float* db, int64_t M, int N, void* stream);
+int chemgen_mlp_adam(float* w, const float* g, float* m, float* v, void* wb, int64_t n, const float* hyper, float b1,
+                     float b2, float eps, float wd, void* stream);
+int chemgen_surrogate_features(const double* P, const double* T, const double* Y, int64_t ng, int ns, int din,
+                               const float* norm, const double* inv_mw, void* X, float* Xf, void* stream);
+int chemgen_surrogate_targets(const double* W, int64_t ng, int ns, int dout, const float* lnorm, float* Tg,
+                              void* stream);
+int chemgen_surrogate_decode(const float* out, int64_t ng, int ns, int dout, const float* lnorm, double* W,
+                             float* err_est, void* stream);
+
 /* FP64 getrates that allocates no device memory (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc while they run -- a
  * solver that owns the device memory pool or forbids allocation (and the

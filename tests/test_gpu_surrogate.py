@@ -1,0 +1,175 @@
+"""The learned surrogate: kernel products and gradients against the CPU
+oracle, training on samples from the exact kernel, and what the trained
+network gains over the exact kernel alone at its achieved tolerance (judged
+by the FP64 kernel)."""
+import math
+
+import numpy as np
+import pytest
+
+from chemgen_b200 import synthetic
+from chemgen_b200.runtime import GpuMechanism
+
+pytestmark = pytest.mark.gpu
+
+
+def test_mlp_gemm_all_stride_forms():
+    import torch
+    from chemgen_b200.runtime import lib
+    g = torch.Generator(device="cuda").manual_seed(0)
+    A = torch.randn(77, 45, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(33, 45, device="cuda", generator=g).to(torch.bfloat16)
+    s = torch.cuda.current_stream().cuda_stream
+    C = torch.empty(77, 33, device="cuda")
+    assert lib().chemgen_mlp_gemm(A.data_ptr(), 45, 1, B.data_ptr(), 45, 1, C.data_ptr(), 33, 77, 33, 45, 0, s) == 0
+    assert torch.allclose(C, A.float() @ B.float().T, rtol=1e-5, atol=1e-4)
+    # transposed A and B through strides
+    C2 = torch.empty(45, 45, device="cuda")
+    assert lib().chemgen_mlp_gemm(A.data_ptr(), 1, 45, A.data_ptr(), 1, 45, C2.data_ptr(), 45, 45, 45, 77, 0, s) == 0
+    assert torch.allclose(C2, A.float().T @ A.float(), rtol=1e-5, atol=1e-3)
+    # long reductions split over r (atomic slices), overwrite and accumulate, both load orders
+    D = torch.randn(3000, 70, device="cuda", generator=g).to(torch.bfloat16)
+    E = torch.randn(3000, 40, device="cuda", generator=g).to(torch.bfloat16)
+    ref = D.float().T @ E.float()
+    C3 = torch.full((70, 40), 7.0, device="cuda")
+    assert lib().chemgen_mlp_gemm(D.data_ptr(), 1, 70, E.data_ptr(), 1, 40, C3.data_ptr(), 40, 70, 40, 3000, 0, s) == 0
+    assert torch.allclose(C3, ref, rtol=1e-4, atol=1e-2)
+    assert lib().chemgen_mlp_gemm(D.data_ptr(), 1, 70, E.data_ptr(), 1, 40, C3.data_ptr(), 40, 70, 40, 3000, 1, s) == 0
+    assert torch.allclose(C3, 2 * ref, rtol=1e-4, atol=2e-2)
+    Dt, Et = D.T.contiguous(), E.T.contiguous()
+    C4 = torch.empty(70, 40, device="cuda")
+    assert lib().chemgen_mlp_gemm(Dt.data_ptr(), 3000, 1, Et.data_ptr(), 3000, 1, C4.data_ptr(), 40, 70, 40, 3000, 0,
+                                  s) == 0
+    assert torch.allclose(C4, ref, rtol=1e-4, atol=1e-2)
+    # invalid arguments are rejected before any launch
+    assert lib().chemgen_mlp_gemm(0, 1, 1, B.data_ptr(), 1, 1, C.data_ptr(), 33, 1, 1, 1, 0, s) == 1
+    assert lib().chemgen_mlp_gemm(A.data_ptr(), 45, 1, B.data_ptr(), 45, 1, C.data_ptr(), 10, 77, 33, 45, 0, s) == 1
+
+
+@pytest.mark.parametrize("split", [False, True])
+@pytest.mark.parametrize("round_bf16,tol", [(True, 2e-3), (False, 5e-2)])
+def test_kernel_gradients_match_cpu_oracle(round_bf16, tol, split):
+    import torch
+    from chemgen_b200 import surrogate as S
+    from chemgen_b200.runtime import lib
+    from oracle import mlp_ref
+    net = S.MLP(seed=3)
+    B = 192
+    g = torch.Generator(device="cuda").manual_seed(1)
+    F = torch.randn(B, S.DIN, device="cuda", generator=g)
+    if split:
+        # hi + lo BF16 parts; the network's input is their (FP32-exact) sum
+        hi = F.to(torch.bfloat16)
+        lo = (F - hi.float()).to(torch.bfloat16)
+        X = torch.cat([hi, lo], dim=1).contiguous()
+        Xin = hi.float() + lo.float()
+    else:
+        X = F.to(torch.bfloat16)
+        Xin = X.float()
+    tgt = torch.randn(B, S.DOUT, device="cuda", generator=g)
+    colw = torch.ones(S.DOUT, device="cuda")
+    colw[60:] = 0.0
+    for bb in net.b:
+        bb.normal_(0.0, 0.1, generator=g)
+    out = net.forward(X)
+    loss = torch.zeros(1, device="cuda")
+    db = torch.empty(B, S.DOUT, dtype=torch.bfloat16, device="cuda")
+    df = torch.empty(B, S.DOUT, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    assert lib().chemgen_mlp_mse_grad(out.data_ptr(), tgt.data_ptr(), colw.data_ptr(), db.data_ptr(), df.data_ptr(),
+                                      loss.data_ptr(), B, S.DOUT, s) == 0
+    grads = net.backward(db, df)
+    cpu = lambda t: t.detach().cpu().float()
+    o_ref, l_ref, gW, gb = mlp_ref.forward_backward([cpu(w) for w in net.W], [cpu(b) for b in net.b], cpu(Xin),
+                                                    cpu(tgt), cpu(colw), round_bf16=round_bf16)
+    assert (cpu(out) - o_ref).norm() / o_ref.norm() < tol
+    assert abs(loss.item() - l_ref.item()) <= tol * abs(l_ref.item())
+    for got, ref in zip(grads, gW + gb):
+        rel = (cpu(got) - ref).norm() / ref.norm()
+        assert rel < tol, rel.item()
+
+
+def test_features_targets_decode_round_trip():
+    """Split features reproduce the FP32 features to ~2^-16; decode inverts targets."""
+    import torch
+    from chemgen_b200 import surrogate as S
+    from chemgen_b200.runtime import lib
+    gm = GpuMechanism(synthetic.gri_shape())
+    sur = S.Surrogate(gm)
+    P, T, Y = sur.sample_states(5000, torch.Generator(device="cuda").manual_seed(7))
+    sur._set_species_norm(Y)
+    X = torch.empty((5000, 2 * S.DIN), dtype=torch.bfloat16, device="cuda")
+    Xf = torch.empty((5000, S.DIN), device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    assert lib().chemgen_surrogate_features(P.data_ptr(), T.data_ptr(), Y.data_ptr(), 5000, sur.ns, S.DIN,
+                                            sur.norm.data_ptr(), sur.inv_mw.data_ptr(), X.data_ptr(), Xf.data_ptr(),
+                                            s) == 0
+    both = X[:, :S.DIN].float() + X[:, S.DIN:].float()
+    assert ((both - Xf).abs() <= Xf.abs() * 2.0 ** -15 + 1e-30).all()
+    # features against a torch restatement (FP64 before the FP32 rounding)
+    Xm = Y.clamp_min(1e-30) * sur.inv_mw[:, None]
+    lx = torch.log(Xm) - torch.log(Xm.sum(dim=0, keepdim=True))
+    ref = ((lx - sur.norm[6].double()) * sur.norm[7].double()).clamp(-6, 6).T
+    assert torch.allclose(Xf[:, 3:3 + sur.ns].double(), ref, atol=1e-5)
+    assert torch.allclose(Xf[:, 0].double(), (1000.0 / T - 1.3) / 0.9, atol=1e-5)
+    assert (Xf[:, 3 + sur.ns:] == 0).all()
+    W = gm.getrates(P, T, Y)
+    ln_n = torch.log(W.norm(dim=0))
+    sur.lnorm[0], sur.lnorm[1] = float(ln_n.mean()), float(ln_n.std())
+    Tg = sur.targets(W)
+    assert torch.allclose(Tg[:, :sur.ns].double().norm(dim=1), torch.ones(5000, dtype=torch.float64, device="cuda"),
+                          atol=1e-5)
+    Tg[:, sur.ns + 1] = -3.0
+    W2, est = sur.decode(Tg)
+    assert ((W2 - W).abs().max(dim=0).values / W.abs().max(dim=0).values).max() < 1e-5
+    assert (est == -3.0).all()
+
+
+def test_surrogate_trains_and_gains_over_exact_kernel():
+    import torch
+    from chemgen_b200 import surrogate as S
+    mech = synthetic.gri_shape()
+    gm = GpuMechanism(mech, generated=True)
+    sur = S.Surrogate(gm, seed=0)
+    info = sur.fit(S.TrainConfig(samples=4_000_000, batch=2048, epochs=12, error_head_epochs=1))
+    print(info, sur.history)
+    assert sur.history[-1] < 0.05 * sur.history[0]
+    # held-out states, judged by the FP64 kernel
+    ng = 1 << 18
+    gen = torch.Generator(device="cuda").manual_seed(99)
+    P, T, Y = sur.sample_states(ng, gen)
+    W64 = gm.getrates(P, T, Y, mode="fp64")
+    Wsur, est = sur.predict(P, T, Y)
+    err = ((Wsur - W64).abs().max(dim=0).values / W64.abs().max(dim=0).values).cpu().numpy()
+    med = float(np.median(err))
+    print("held-out normwise error: median", med, "p90", np.quantile(err, 0.9))
+    assert med < 0.1, med
+    # the error estimate ranks points: accepted points are more accurate than rejected ones
+    tol = float(np.quantile(err, 0.5))
+    run = S.SurrogateGetrates(sur, tol=tol)
+    W = run(P, T, Y)
+    ok = (est <= math.log10(tol)).cpu().numpy()
+    assert 0.0 < run.last_fallback < 1.0
+    assert np.median(err[ok]) < np.median(err[~ok])
+    # fallback points carry the exact kernel's values
+    e_after = ((W - W64).abs().max(dim=0).values / W64.abs().max(dim=0).values).cpu().numpy()
+    assert (e_after[~ok] < 1e-5).all()
+    assert np.quantile(e_after, 0.9) <= np.quantile(err, 0.9)
+
+
+def test_checkpoint_round_trip(tmp_path):
+    import torch
+    from chemgen_b200 import surrogate as S
+    gm = GpuMechanism(synthetic.gri_shape())
+    a = S.Surrogate(gm, seed=0)
+    a.fit(S.TrainConfig(samples=1 << 16, batch=2048, epochs=1, error_head_epochs=1))
+    a.save(str(tmp_path / "sur.pt"))
+    b = S.Surrogate(gm, seed=5)
+    b.load(str(tmp_path / "sur.pt"))
+    P, T, Y = a.sample_states(4096, torch.Generator(device="cuda").manual_seed(3))
+    wa, ea = a.predict(P, T, Y)
+    wb, eb = b.predict(P, T, Y)
+    assert torch.equal(wa, wb) and torch.equal(ea, eb)
+    other = GpuMechanism(synthetic.h2o2_10sp())
+    with pytest.raises(ValueError):
+        S.Surrogate(other).load(str(tmp_path / "sur.pt"))
