@@ -10,7 +10,7 @@
 //   strides, so one kernel serves the forward product (X W^T), the input
 //   gradient (dZ W) and the weight gradient (dZ^T H); long reductions over
 //   few output tiles (weight gradients) are split over r;
-// * elementwise kernels: bias + GELU (tanh form) forward, GELU backward, loss
+// * elementwise kernels: bias + GELU (tanh form, hardware tanh) forward, GELU backward, loss
 //   gradient, column sums for bias gradients, Adam with FP32 master weights;
 // * the feature / target transforms between (P, T, Y, wdot) and network
 //   space, and the decode of predictions back to wdot.
@@ -137,13 +137,24 @@ __global__ void __launch_bounds__(128) mlp_gemm_kernel(const bf16* __restrict__ 
                 }
 }
 
-// GELU, tanh form: 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))
+// The network's activation: GELU in tanh form,
+// 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))), with tanh from the
+// hardware approximation (tanh.approx.f32, relative error about 2^-11).  The
+// same function is evaluated in training and in the fused inference kernel,
+// so the trained weights are exact for it.
+__device__ __forceinline__ float tanh_hw(float u) {
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+    return t;
+}
+
 __device__ __forceinline__ float gelu(float z, float* dgelu) {
     const float k0 = 0.7978845608028654f, k1 = 0.044715f;
     const float u = k0 * fmaf(k1 * z * z, z, z);
-    const float t = tanhf(u);
+    const float t = tanh_hw(u);
     if (dgelu) *dgelu = 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * k0 * fmaf(3.0f * k1, z * z, 1.0f);
-    return 0.5f * z * (1.0f + t);
+    const float hz = 0.5f * z;
+    return fmaf(hz, t, hz);
 }
 
 // Z[m][n] += bias[n]; H = GELU(Z) as BF16 (and FP32 Z kept for the backward)

@@ -1,0 +1,400 @@
+// Fused inference of the wdot surrogate on the 5th-generation tensor cores:
+// features -> 4 MLP layers -> decoded FP64 wdot in one kernel, activations
+// never leaving the SM.
+//
+// One persistent CTA of 256 threads per SM works through tiles of 128 points:
+// * features: each point's 64 network inputs (1000/T, ln T, ln P/1 atm,
+//   ln X_k, zeros), centred and scaled, split into BF16 hi + lo parts, are
+//   written straight into the shared-memory A operand [128 x 128] in the
+//   K-major canonical layout;
+// * layer l: one thread issues K/16 tcgen05.mma (M = 128, N = 256 or 64,
+//   K = 16, BF16 in, FP32 accumulate in tensor memory) against the layer's
+//   weights, which a bulk asynchronous copy (cp.async.bulk, no multicast)
+//   brought into shared memory while the previous epilogue ran;
+// * epilogue l < 3: tcgen05.ld of the accumulators, bias, GELU (tanh form,
+//   hardware tanh as in training), BF16, back into the A operand of the next
+//   layer (K = 256);
+// * epilogue l = 3: w_k = (u_k + b_k) exp(c + s (L + b_L)) in FP64, stored
+//   species-major, and the error estimate.
+// The weights come pre-arranged in the canonical layout (chemgen_surrogate_pack),
+// so every weight load is a straight 16-byte-aligned bulk copy.  Shared
+// memory: 64 KB activations + 128 KB weights; tensor memory: 256 columns.
+// Every mbarrier wait is bounded; a time-out sets the error word and the
+// kernel drains what it issued before freeing tensor memory.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+
+#include "../../include/chemgen_b200.h"
+#include "umma.cuh"
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int kPts = 128, kThreads = 256;
+constexpr int kDin = 64, kK1 = 2 * kDin, kHid = 256, kDout = 64;
+constexpr int kW1 = kHid * kK1, kW2 = kHid * kHid, kW4 = kDout * kHid;
+constexpr int kImgElems = kW1 + 2 * kW2 + kW4;
+constexpr int kBiasElems = 3 * kHid + kDout;
+constexpr uint32_t kABytes = kPts * kHid * 2;
+constexpr uint32_t kWBytes = kHid * kHid * 2;
+constexpr uint32_t kTailOff = kABytes + kWBytes;            // barriers, flags, TMEM slot (64 B)
+constexpr uint32_t kPartOff = kTailOff + 64;                 // [2][128] partial mixture sums
+constexpr uint32_t kBiasOff = kPartOff + 2 * kPts * 4;       // [832] biases
+constexpr size_t kSmem = (size_t)kBiasOff + kBiasElems * 4;
+constexpr uint32_t kCopyPiece = 16384;
+
+__device__ int g_sur_err;
+
+__host__ __device__ constexpr int layer_k(int l) { return l == 0 ? kK1 : kHid; }
+__host__ __device__ constexpr int layer_n(int l) { return l == 3 ? kDout : kHid; }
+__host__ __device__ constexpr int layer_off(int l) {
+    return l == 0 ? 0 : l == 1 ? kW1 : l == 2 ? kW1 + kW2 : kW1 + 2 * kW2;
+}
+
+__device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
+    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+// The network's activation exactly as in training (chemgen_mlp_bias_gelu):
+// GELU in tanh form with the hardware tanh approximation, one MUFU operation.
+__device__ __forceinline__ float gelu_fast(float z) {
+    const float u = 0.7978845608028654f * fmaf(0.044715f * z * z, z, z);
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+    const float hz = 0.5f * z;
+    return fmaf(hz, t, hz);
+}
+
+__device__ __forceinline__ void gelu_store16(const uint32_t* r, const float* b, unsigned char* dst0,
+                                             unsigned char* dst1) {
+    uint32_t pk[8];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float4 bb = *reinterpret_cast<const float4*>(b + 4 * q);
+        const float z0 = __uint_as_float(r[4 * q]) + bb.x, z1 = __uint_as_float(r[4 * q + 1]) + bb.y;
+        const float z2 = __uint_as_float(r[4 * q + 2]) + bb.z, z3 = __uint_as_float(r[4 * q + 3]) + bb.w;
+        pk[2 * q] = pack2(__float2bfloat16(gelu_fast(z0)), __float2bfloat16(gelu_fast(z1)));
+        pk[2 * q + 1] = pack2(__float2bfloat16(gelu_fast(z2)), __float2bfloat16(gelu_fast(z3)));
+    }
+    *reinterpret_cast<uint4*>(dst0) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    *reinterpret_cast<uint4*>(dst1) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+}
+
+__device__ __forceinline__ void issue_weights(const bf16* img, int l, unsigned char* sW, uint64_t* wbar) {
+    const uint32_t bytes = (uint32_t)layer_n(l) * layer_k(l) * 2;
+    um::mbar_expect_tx(wbar, bytes);
+    const unsigned char* src = reinterpret_cast<const unsigned char*>(img + layer_off(l));
+    for (uint32_t o = 0; o < bytes; o += kCopyPiece) um::bulk_g2s(sW + o, src + o, kCopyPiece, wbar);
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    surrogate_infer_kernel(const bf16* __restrict__ img, const float* __restrict__ bias,
+                           const float* __restrict__ norm, const float* __restrict__ lnorm,
+                           const double* __restrict__ inv_mw, int ns, const double* __restrict__ P,
+                           const double* __restrict__ T, const double* __restrict__ Y, int64_t ng,
+                           double* __restrict__ W, float* __restrict__ est) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    unsigned char* sA = sm;
+    unsigned char* sW = sm + kABytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kTailOff);          // [0] MMAs done, [1] weights landed
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
+    volatile int* wfail = reinterpret_cast<volatile int*>(bars + 3);       // set by thread 0 before a barrier
+    volatile int* mfail = wfail + 1;                                        // set after the MMA wait
+    float* sPart = reinterpret_cast<float*>(sm + kPartOff);
+    float* sBias = reinterpret_cast<float*>(sm + kBiasOff);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t ntiles = (ng + kPts - 1) / kPts;
+    if (tid == 0) {
+        um::mbar_init(&bars[0], 1);
+        um::mbar_init(&bars[1], 1);
+        *wfail = 0;
+        *mfail = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int q = tid; q < kBiasElems; q += kThreads) sBias[q] = __ldg(bias + q);
+    if (warp == 0) um::tmem_alloc(tslot, 256);
+    um::fence_before_sync();
+    __syncthreads();
+    um::fence_after_sync();
+    const uint32_t tbase = *tslot;
+    float nrm[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) nrm[q] = __ldg(norm + q);
+    const double lc = (double)__ldg(lnorm), ls = (double)__ldg(lnorm + 1);
+    uint32_t mpar = 0, wpar = 0;
+    bool w_pending = false, m_failed = false;
+    if (tid == 0) {
+        issue_weights(img, 0, sW, &bars[1]);
+        w_pending = true;
+    }
+    const int row = tid & (kPts - 1), half = tid >> 7;  // features: point, which 32 inputs
+    const int g4 = warp & 3, ehalf = warp >> 2;         // epilogue: TMEM lane group, column half
+    const int erow = 32 * g4 + lane;
+    bool failed = false;
+    for (int64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+        // the next tile's inputs start moving into L2 now
+        if (warp == 7 && tile + gridDim.x < ntiles) {
+            const int64_t n0 = (tile + gridDim.x) * kPts;
+            const uint32_t bytes = (uint32_t)(min((int64_t)kPts, ng - n0) * 8) & ~15u;
+            for (int r = lane; r < ns + 2 && bytes; r += 32) {
+                const double* src = r < ns ? Y + (int64_t)r * ng + n0 : (r == ns ? T + n0 : P + n0);
+                if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) um::bulk_prefetch_l2(src, bytes);
+            }
+        }
+        // ---- features -> A [128 x 128].  Thread (row, half) owns inputs
+        // 32 half .. 32 half + 31 of point `row`: it loads all of its mass
+        // fractions at once, and the two halves add their parts of
+        // sum_k Y_k / W_k through shared memory.
+        {
+            const int64_t i = tile * kPts + row;
+            const bool act = i < ng;
+            const int jb = 32 * half;
+            // unconditional loads from clamped (always valid) indices, so that
+            // all 32 are in flight together; out-of-range values become 0
+            const int64_t ic = act ? i : ng - 1;
+            float y[32];
+#pragma unroll
+            for (int u = 0; u < 32; ++u) {
+                const int k = jb + u - 3;
+                const int kc = min(max(k, 0), ns - 1);
+                const float v = (float)__ldg(Y + (int64_t)kc * ng + ic);
+                y[u] = (act && k >= 0 && k < ns) ? v : 0.0f;
+            }
+            float invT = 0.0f, lnT = 0.0f, lnP = 0.0f;
+            if (act && half == 0) {
+                const double t = T[i];
+                invT = (float)(1000.0 / t);
+                lnT = logf((float)t);
+                lnP = logf((float)(P[i] / 1013250.0));
+            }
+            float part = 0.0f;
+#pragma unroll
+            for (int u = 0; u < 32; ++u) {
+                const int k = jb + u - 3;
+                if (k >= 0 && k < ns) part = fmaf(fmaxf(y[u], 0.0f), (float)__ldg(inv_mw + k), part);
+            }
+            sPart[half * kPts + row] = part;
+            __syncthreads();
+            const float lmix = __logf(fmaxf(sPart[row] + sPart[kPts + row], 1e-37f));
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+                uint32_t hi[4], lo[4];
+#pragma unroll
+                for (int u = 0; u < 8; u += 2) {
+                    float f[2];
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const int uu = 8 * g + u + e, j = jb + uu, k = j - 3;
+                        float v = 0.0f;
+                        if (act) {
+                            if (j == 0) {
+                                v = (invT - nrm[0]) * nrm[1];
+                            } else if (j == 1) {
+                                v = (lnT - nrm[2]) * nrm[3];
+                            } else if (j == 2) {
+                                v = (lnP - nrm[4]) * nrm[5];
+                            } else if (k < ns) {
+                                // fast log: ~1e-5 absolute, below the ~2^-16 of the split inputs
+                                const float lx = __logf(fmaxf(y[uu], 1e-30f) * (float)__ldg(inv_mw + k)) - lmix;
+                                v = fminf(fmaxf((lx - nrm[6]) * nrm[7], -6.0f), 6.0f);
+                            }
+                        }
+                        f[e] = v;
+                    }
+                    const bf16 h0 = __float2bfloat16(f[0]), h1 = __float2bfloat16(f[1]);
+                    hi[u / 2] = pack2(h0, h1);
+                    lo[u / 2] = pack2(__float2bfloat16(f[0] - __bfloat162float(h0)),
+                                      __float2bfloat16(f[1] - __bfloat162float(h1)));
+                }
+                const int j0 = jb + 8 * g;
+                *reinterpret_cast<uint4*>(sA + um::kmajor_offset(row, j0, kK1)) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+                *reinterpret_cast<uint4*>(sA + um::kmajor_offset(row, kDin + j0, kK1)) =
+                    make_uint4(lo[0], lo[1], lo[2], lo[3]);
+            }
+        }
+        um::fence_proxy_async();
+        um::fence_before_sync();
+        __syncthreads();
+        um::fence_after_sync();
+        for (int l = 0; l < 4; ++l) {
+            const int K = layer_k(l), N = layer_n(l);
+            if (tid == 0) {
+                const bool ok = um::mbar_wait(&bars[1], wpar);
+                if (ok) {
+                    wpar ^= 1u;
+                    w_pending = false;
+                    um::fence_after_sync();
+                    const uint32_t idesc = um::idesc_bf16(kPts, N);
+                    const uint32_t a = um::smem_addr(sA), b = um::smem_addr(sW);
+                    for (int ks = 0; ks < K / 16; ++ks)
+                        um::mma_bf16(tbase, um::desc_kmajor(a, K, ks), um::desc_kmajor(b, K, ks), idesc,
+                                     ks > 0 ? 1u : 0u);
+                    um::commit(&bars[0]);
+                } else {
+                    *wfail = 1;
+                }
+            }
+            __syncthreads();
+            if (*wfail) {
+                failed = true;
+                break;
+            }
+            const bool ok = um::mbar_wait(&bars[0], mpar);
+            if (!ok) {
+                *mfail = 1;
+                m_failed = true;
+            } else {
+                mpar ^= 1u;
+            }
+            um::fence_after_sync();
+            if (ok) {
+                // the weights of the next layer (or of the next tile's first
+                // layer) stream in while this epilogue runs
+                if (tid == 0 && (l < 3 || tile + gridDim.x < ntiles)) {
+                    issue_weights(img, l < 3 ? l + 1 : 0, sW, &bars[1]);
+                    w_pending = true;
+                }
+                if (l < 3) {
+                    const float* bl = sBias + kHid * l;
+#pragma unroll 1
+                    for (int c = 128 * ehalf; c < 128 * ehalf + 128; c += 32) {
+                        uint32_t ra[16], rb[16];
+                        um::tmem_ld16_nowait(um::tmem_lane_addr(tbase, g4, c), ra);
+                        um::tmem_ld16_nowait(um::tmem_lane_addr(tbase, g4, c + 16), rb);
+                        um::tmem_wait_ld(ra);
+                        um::tmem_wait_ld(rb);
+                        gelu_store16(ra, bl + c, sA + um::kmajor_offset(erow, c, kHid),
+                                     sA + um::kmajor_offset(erow, c + 8, kHid));
+                        gelu_store16(rb, bl + c + 16, sA + um::kmajor_offset(erow, c + 16, kHid),
+                                     sA + um::kmajor_offset(erow, c + 24, kHid));
+                    }
+                } else {
+                    const float* b4 = sBias + 3 * kHid;
+                    const int64_t i = tile * kPts + erow;
+                    const bool act = i < ng;
+                    const int cL = (ns / 16) * 16;
+                    float v[16];
+                    um::tmem_ld16(um::tmem_lane_addr(tbase, g4, cL), v);
+                    float L = 0.0f;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        if (cL + j == ns) L = v[j];
+                    const double scale = exp(lc + ls * (double)(L + b4[ns]));
+#pragma unroll 1
+                    for (int c = 32 * ehalf; c < 32 * ehalf + 32; c += 16) {
+                        um::tmem_ld16(um::tmem_lane_addr(tbase, g4, c), v);
+                        if (act) {
+#pragma unroll
+                            for (int j = 0; j < 16; ++j) {
+                                const int k = c + j;
+                                if (k < ns) W[(int64_t)k * ng + i] = (double)(v[j] + b4[k]) * scale;
+                                else if (k == ns + 1 && est) est[i] = v[j] + b4[k];
+                            }
+                        }
+                    }
+                }
+            }
+            um::fence_proxy_async();
+            um::fence_before_sync();
+            __syncthreads();
+            um::fence_after_sync();
+            if (*mfail) {
+                failed = true;
+                break;
+            }
+        }
+    }
+    if (failed) {
+        // drain what this CTA issued (bounded) before tensor memory is freed
+        if (tid == 0) {
+            atomicExch(&g_sur_err, 1);
+            if (w_pending) um::mbar_wait(&bars[1], wpar);
+        }
+        if (m_failed) um::mbar_wait(&bars[0], mpar);
+    }
+    um::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) um::tmem_dealloc(tbase, 256);
+}
+
+// Weight image: layer l's [N_l x K_l] BF16 operand in the K-major canonical
+// layout (element (n, k) at (n/8) K 8 + (k/8) 64 + (n%8) 8 + k%8), layers
+// back to back; layer 0's K = 128 holds the 64 input weights twice (for the
+// hi and lo parts of the inputs).
+__global__ void pack_kernel(const bf16* __restrict__ W1, const bf16* __restrict__ W2, const bf16* __restrict__ W3,
+                            const bf16* __restrict__ W4, bf16* __restrict__ img) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= kImgElems) return;
+    const int l = d < layer_off(1) ? 0 : d < layer_off(2) ? 1 : d < layer_off(3) ? 2 : 3;
+    const int K = layer_k(l), local = d - layer_off(l);
+    const int rg = local / (K * 8), rem = local % (K * 8);
+    const int kc = rem / 64, r8 = (rem % 64) / 8, k8 = rem % 8;
+    const int n = rg * 8 + r8, k = kc * 8 + k8;
+    bf16 v;
+    if (l == 0) v = W1[n * kDin + (k % kDin)];
+    else if (l == 1) v = W2[n * kHid + k];
+    else if (l == 2) v = W3[n * kHid + k];
+    else v = W4[n * kHid + k];
+    img[d] = v;
+}
+
+int sm_count() {
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    return n;
+}
+
+}  // namespace
+
+extern "C" {
+
+int chemgen_surrogate_image_elems(void) { return kImgElems; }
+
+int chemgen_surrogate_pack(const void* W1, const void* W2, const void* W3, const void* W4, void* img, void* stream) {
+    if (!W1 || !W2 || !W3 || !W4 || !img) return CHEMGEN_ERR_INVALID_ARGUMENT;
+    if (reinterpret_cast<uintptr_t>(img) & 15) return CHEMGEN_ERR_MISALIGNED;
+    pack_kernel<<<(kImgElems + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        (const bf16*)W1, (const bf16*)W2, (const bf16*)W3, (const bf16*)W4, (bf16*)img);
+    return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA;
+}
+
+int chemgen_surrogate_infer(const void* img, const float* bias, const float* norm, const float* lnorm,
+                            const double* inv_mw, int ns, const double* P, const double* T, int64_t ng,
+                            const double* Y, double* wdot, float* err_est, void* stream) {
+    if (!img || !bias || !norm || !lnorm || !inv_mw || !P || !T || !Y || !wdot || ng < 0)
+        return CHEMGEN_ERR_INVALID_ARGUMENT;
+    if (ns < 1 || ns + 3 > kDin || ns + 2 > kDout) return CHEMGEN_ERR_UNSUPPORTED;
+    if (reinterpret_cast<uintptr_t>(img) & 15) return CHEMGEN_ERR_MISALIGNED;
+    if (ng == 0) return CHEMGEN_OK;
+    static std::mutex mu;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (cudaFuncSetAttribute(surrogate_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem) !=
+            cudaSuccess)
+            return CHEMGEN_ERR_CUDA;
+    }
+    const int sms = sm_count();
+    if (sms <= 0) return CHEMGEN_ERR_CUDA;
+    const int64_t ntiles = (ng + kPts - 1) / kPts;
+    const unsigned grid = (unsigned)(ntiles < sms ? ntiles : sms);
+    surrogate_infer_kernel<<<grid, kThreads, kSmem, (cudaStream_t)stream>>>(
+        (const bf16*)img, bias, norm, lnorm, inv_mw, ns, P, T, Y, ng, wdot, err_est);
+    return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA;
+}
+
+int chemgen_surrogate_infer_error(int reset) {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_sur_err, sizeof(int)) != cudaSuccess) return -1;
+    if (reset && v) {
+        const int z = 0;
+        if (cudaMemcpyToSymbol(g_sur_err, &z, sizeof(int)) != cudaSuccess) return -1;
+    }
+    return v;
+}
+
+}  // extern "C"

@@ -77,9 +77,14 @@ def lib() -> ctypes.CDLL:
     L.chemgen_surrogate_features.argtypes = [vp, vp, vp, i64, ci, ci, vp, vp, vp, vp, vp]
     L.chemgen_surrogate_targets.argtypes = [vp, i64, ci, ci, vp, vp, vp]
     L.chemgen_surrogate_decode.argtypes = [vp, i64, ci, ci, vp, vp, vp, vp]
+    L.chemgen_surrogate_image_elems.argtypes = []
+    L.chemgen_surrogate_pack.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.chemgen_surrogate_infer.argtypes = [vp, vp, vp, vp, vp, ci, vp, vp, i64, vp, vp, vp, vp]
+    L.chemgen_surrogate_infer_error.argtypes = [ci]
     for f in ("chemgen_mlp_gemm", "chemgen_mlp_bias_gelu", "chemgen_mlp_gelu_backward", "chemgen_mlp_mse_grad",
               "chemgen_mlp_colsum", "chemgen_mlp_adam", "chemgen_surrogate_features", "chemgen_surrogate_targets",
-              "chemgen_surrogate_decode"):
+              "chemgen_surrogate_decode", "chemgen_surrogate_image_elems", "chemgen_surrogate_pack",
+              "chemgen_surrogate_infer", "chemgen_surrogate_infer_error"):
         getattr(L, f).restype = ci
     L.chemgen_use_generated.argtypes = [vp, ci]
     L.chemgen_kernel_kind.argtypes = [vp, ci]

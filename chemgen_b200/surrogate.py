@@ -202,6 +202,7 @@ class Surrogate:
         self.T_range = (300.0, 2500.0)
         self.P_range = (1013250.0, 1013250.0 * 40.0)
         self.history: List[float] = []
+        self._img = None
 
     # ------------------------------------------------------------ transforms
     def features(self, P, T, Y):
@@ -346,6 +347,7 @@ class Surrogate:
         self.fit_error_head(X, Tg, cfg, gen, log)
         torch.cuda.synchronize(self.dev)
         t_head = time.perf_counter() - t2
+        self._img = None
         return {"samples": n, "t_data_s": t_data, "t_train_s": t_train, "t_error_head_s": t_head,
                 "steps": step, "final_loss": self.history[-1] if self.history else None}
 
@@ -420,6 +422,7 @@ class Surrogate:
             self.net.b[l].copy_(st["b"][l].to(self.dev))
         self.norm.copy_(st["norm"].to(self.dev))
         self.lnorm.copy_(st["lnorm"].to(self.dev))
+        self._img = None
 
     def save(self, path: str) -> None:
         import torch
@@ -430,9 +433,39 @@ class Surrogate:
         self.load_state_dict(torch.load(path, map_location="cpu"))
 
     # ------------------------------------------------------------- inference
-    def predict(self, P, T, Y, chunk: int = 1 << 20):
-        """(wdot [ns, ng] FP64, log10 error estimate [ng])."""
+    def packed(self):
+        """(weight image, biases) of the fused inference kernel, built from
+        the current BF16 weights."""
         import torch
+        if self._img is None:
+            img = torch.empty(lib().chemgen_surrogate_image_elems(), dtype=torch.bfloat16, device=self.dev)
+            Wb = self.net.Wb
+            check(lib().chemgen_surrogate_pack(Wb[0].data_ptr(), Wb[1].data_ptr(), Wb[2].data_ptr(), Wb[3].data_ptr(),
+                                               img.data_ptr(), _stream()), "surrogate_pack")
+            self._img = (img, torch.cat(self.net.b).contiguous())
+        return self._img
+
+    def predict_fused(self, P, T, Y, out=None, est=None):
+        """(wdot [ns, ng] FP64, log10 error estimate [ng]) from the fused
+        tensor-core kernel (one launch)."""
+        import torch
+        ng = T.numel()
+        img, bias = self.packed()
+        W = out if out is not None else torch.empty((self.ns, ng), dtype=torch.float64, device=self.dev)
+        e = est if est is not None else torch.empty(ng, dtype=torch.float32, device=self.dev)
+        check(lib().chemgen_surrogate_infer(img.data_ptr(), bias.data_ptr(), self.norm.data_ptr(),
+                                            self.lnorm.data_ptr(), self.inv_mw.data_ptr(), self.ns, P.data_ptr(),
+                                            T.data_ptr(), ng, Y.data_ptr(), W.data_ptr(), e.data_ptr(), _stream()),
+              "surrogate_infer")
+        return W, e
+
+    def predict(self, P, T, Y, chunk: int = 1 << 20, fused: bool = True):
+        """(wdot [ns, ng] FP64, log10 error estimate [ng]); `fused` selects
+        the one-kernel tensor-core path, otherwise the layer-by-layer kernels
+        used in training."""
+        import torch
+        if fused:
+            return self.predict_fused(P.contiguous(), T.contiguous(), Y.contiguous())
         ng = T.numel()
         W = torch.empty((self.ns, ng), dtype=torch.float64, device=self.dev)
         est = torch.empty(ng, dtype=torch.float32, device=self.dev)

@@ -148,6 +148,25 @@ int chemgen_surrogate_targets(const double* W, int64_t ng, int ns, int dout, con
 int chemgen_surrogate_decode(const float* out, int64_t ng, int ns, int dout, const float* lnorm, double* W,
                              float* err_est, void* stream);
 
+/* Fused surrogate inference on the tensor cores (no counterpart in the
+ * reference): features, the four layers (tcgen05.mma, activations kept in
+ * shared and tensor memory) and the decode to FP64 wdot in one kernel, for the
+ * network above with din = 64, hidden 256, dout = 64 and ns <= 61.
+ * chemgen_surrogate_pack: W1 [256 x 64], W2, W3 [256 x 256], W4 [64 x 256] (BF16, row-major
+ *   [out x in]) -> img (chemgen_surrogate_image_elems() BF16 elements, 16-byte aligned), the
+ *   operands in the tensor cores' K-major canonical layout, layer 1 with its input weights twice.
+ * chemgen_surrogate_infer: wdot[k*ng + i] and err_est[i] (may be NULL) from (P, T, Y) with bias =
+ *   (b1, b2, b3 [256 each], b4 [64]), norm[8], lnorm[2] and inv_mw[ns] as in
+ *   chemgen_surrogate_features / _decode.  Asynchronous on `stream`.
+ * chemgen_surrogate_infer_error: 1 if a bounded wait inside the kernel ever gave up (its outputs
+ *   are then incomplete), 0 otherwise, -1 on a CUDA error; synchronous; reset != 0 clears it. */
+int chemgen_surrogate_image_elems(void);
+int chemgen_surrogate_pack(const void* W1, const void* W2, const void* W3, const void* W4, void* img, void* stream);
+int chemgen_surrogate_infer(const void* img, const float* bias, const float* norm, const float* lnorm,
+                            const double* inv_mw, int ns, const double* P, const double* T, int64_t ng,
+                            const double* Y, double* wdot, float* err_est, void* stream);
+int chemgen_surrogate_infer_error(int reset);
+
 /* FP64 getrates that allocates no device memory (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc while they run -- a
  * solver that owns the device memory pool or forbids allocation (and the

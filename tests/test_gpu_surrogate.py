@@ -46,8 +46,12 @@ def test_mlp_gemm_all_stride_forms():
     assert lib().chemgen_mlp_gemm(A.data_ptr(), 45, 1, B.data_ptr(), 45, 1, C.data_ptr(), 10, 77, 33, 45, 0, s) == 1
 
 
+# The kernels' GELU uses the hardware tanh approximation (relative error
+# about 2^-11); the oracle uses exact tanh.  With the BF16 roundings
+# restated, what is left is that approximation moving a fraction of the
+# activations across a BF16 rounding boundary: well under 5e-3 in norm.
 @pytest.mark.parametrize("split", [False, True])
-@pytest.mark.parametrize("round_bf16,tol", [(True, 2e-3), (False, 5e-2)])
+@pytest.mark.parametrize("round_bf16,tol", [(True, 5e-3), (False, 5e-2)])
 def test_kernel_gradients_match_cpu_oracle(round_bf16, tol, split):
     import torch
     from chemgen_b200 import surrogate as S
@@ -155,6 +159,74 @@ def test_surrogate_trains_and_gains_over_exact_kernel():
     e_after = ((W - W64).abs().max(dim=0).values / W64.abs().max(dim=0).values).cpu().numpy()
     assert (e_after[~ok] < 1e-5).all()
     assert np.quantile(e_after, 0.9) <= np.quantile(err, 0.9)
+
+
+@pytest.fixture(scope="module")
+def small_surrogate():
+    """A briefly trained network (realistic weight and output scales)."""
+    from chemgen_b200 import surrogate as S
+    gm = GpuMechanism(synthetic.gri_shape())
+    sur = S.Surrogate(gm, seed=1)
+    sur.fit(S.TrainConfig(samples=1 << 18, batch=1024, epochs=2, error_head_epochs=1))
+    return sur
+
+
+def test_weight_image_is_the_canonical_layout(small_surrogate):
+    import torch
+    from chemgen_b200.runtime import lib
+    sur = small_surrogate
+    img, bias = sur.packed()
+    Wb = sur.net.Wb
+
+    def canon(w):   # [N, K] -> (N/8, K/8, 8, 8) core matrices, flattened
+        n, k = w.shape
+        return w.reshape(n // 8, 8, k // 8, 8).permute(0, 2, 1, 3).reshape(-1)
+
+    ref = torch.cat([canon(torch.cat([Wb[0], Wb[0]], dim=1)), canon(Wb[1]), canon(Wb[2]), canon(Wb[3])])
+    assert img.numel() == lib().chemgen_surrogate_image_elems() == ref.numel()
+    assert torch.equal(img, ref)
+    assert torch.equal(bias, torch.cat(sur.net.b))
+
+
+@pytest.mark.parametrize("ng", [1, 1000, 128 * 300 + 5])
+def test_fused_inference_matches_layer_by_layer(small_surrogate, ng):
+    import torch
+    from chemgen_b200.runtime import lib
+    sur = small_surrogate
+    assert lib().chemgen_surrogate_infer_error(1) == 0
+    P, T, Y = sur.sample_states(ng, torch.Generator(device="cuda").manual_seed(ng))
+    W1, e1 = sur.predict(P, T, Y, fused=False)
+    W2, e2 = sur.predict(P, T, Y, fused=True)
+    torch.cuda.synchronize()
+    assert lib().chemgen_surrogate_infer_error(0) == 0
+    # same network and inputs; they differ only where an activation's BF16
+    # rounding falls the other way (FP32 vs FP64 logs in the features, the
+    # summation order of the products): one such flip moves the log-length
+    # output by ~1e-3,
+    # i.e. a few % of wdot at that point, neither path being the exact one
+    rel = ((W2 - W1).abs().max(dim=0).values / W1.abs().max(dim=0).values).cpu().numpy()
+    assert np.isfinite(rel).all()
+    assert np.median(rel) < 1e-4 and np.quantile(rel, 0.99) < 1e-2 and rel.max() < 0.1, \
+        (np.median(rel), np.quantile(rel, 0.99), rel.max())
+    assert (e2 - e1).abs().max().item() < 0.05
+
+
+def test_fused_inference_rejects_bad_arguments(small_surrogate):
+    import torch
+    from chemgen_b200.runtime import lib
+    sur = small_surrogate
+    img, bias = sur.packed()
+    P, T, Y = sur.sample_states(16, torch.Generator(device="cuda").manual_seed(0))
+    W = torch.empty((sur.ns, 16), dtype=torch.float64, device="cuda")
+    args = [bias.data_ptr(), sur.norm.data_ptr(), sur.lnorm.data_ptr(), sur.inv_mw.data_ptr()]
+    s = torch.cuda.current_stream().cuda_stream
+    call = lambda im, ns, ng: lib().chemgen_surrogate_infer(im, *args, ns, P.data_ptr(), T.data_ptr(), ng,
+                                                            Y.data_ptr(), W.data_ptr(), 0, s)
+    assert call(0, sur.ns, 16) == 1
+    assert call(img.data_ptr(), 62, 16) == 6       # more species than outputs
+    assert call(img.data_ptr() + 2, sur.ns, 16) == 5
+    assert call(img.data_ptr(), sur.ns, -1) == 1
+    assert call(img.data_ptr(), sur.ns, 0) == 0
 
 
 def test_checkpoint_round_trip(tmp_path):
