@@ -12,6 +12,12 @@ reported beside it.  Under torchrun every rank runs its own 2^20 points
 (weak scaling, no collective on the data path); times are the max over
 ranks.  `--impl reference` times the FP64 CPU restatement of the reference's
 generated getrates on all host cores instead.
+
+On one GPU the line also carries `surrogate`: the learned MLP surrogate of
+the same mechanism, trained on exact-kernel samples, evaluated on 2^22
+points -- its normwise error against the FP64 kernel, the fused tensor-core
+inference kernel's points/s, the error gate's fallback rate at
+--surrogate-tol and the gain with fallback over the exact kernels.
 """
 from __future__ import annotations
 
@@ -46,6 +52,12 @@ def parse():
     ap.add_argument("--clock-ms", type=float, default=1500.0, help="length of the clock-sampled timed pass")
     ap.add_argument("--e2e-steps", type=int, default=-1, help="host-path steps (default min(steps, 50))")
     ap.add_argument("--table", action="store_true", help="table-driven kernels instead of the generated ones")
+    ap.add_argument("--surrogate-samples", type=int, default=10_000_000,
+                    help="exact-kernel training samples of the learned surrogate (0 skips the surrogate leg)")
+    ap.add_argument("--surrogate-epochs", type=int, default=16)
+    ap.add_argument("--surrogate-points", type=int, default=1 << 22)
+    ap.add_argument("--surrogate-tol", type=float, default=0.05,
+                    help="normwise tolerance of the surrogate's error gate (points above it fall back)")
     return ap.parse_args()
 
 
@@ -164,6 +176,71 @@ def run_reference(args, rank, world):
 
 
 # ------------------------------------------------------------------ our arm
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """The maximum of a per-rank time over all ranks (every rank calls it)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_mpts(points_per_rank: int, world: int, ms_max: float) -> float:
+    """Mpoints/s of the job: every rank's points over the slowest rank's time."""
+    return points_per_rank * world / (ms_max * 1e-3) / 1e6
+
+
+def rank_states(ns: int, ng: int, rank: int):
+    """The points rank `rank` evaluates: its own seeded draw (weak scaling)."""
+    from chemgen_b200 import synthetic
+    return synthetic.states(ns, ng, seed=1000 + rank)
+
+
+def surrogate_leg(args, gm, stream):
+    """Train the MLP surrogate on exact-kernel samples, then report its
+    accuracy (normwise, judged by the FP64 kernel), the fused kernel's
+    points/s, the error gate's fallback rate and what the surrogate with
+    fallback gains over the exact kernels at that tolerance."""
+    import torch
+    from chemgen_b200 import surrogate as S
+    sur = S.Surrogate(gm, seed=0)
+    info = sur.fit(S.TrainConfig(samples=args.surrogate_samples, epochs=args.surrogate_epochs))
+    n = args.surrogate_points
+    P, T, Y = sur.sample_states(n, torch.Generator(device="cuda").manual_seed(4242))
+    W64 = torch.empty((gm.ns, n), dtype=torch.float64, device="cuda")
+    W = torch.empty_like(W64)
+    est = torch.empty(n, dtype=torch.float32, device="cuda")
+    steps = max(3, min(args.steps, 20))
+    ms_fp64 = time_steps(lambda: gm.getrates(P, T, Y, out=W64, mode="fp64", stream=stream), steps, 3, stream)
+    ms_mixed = time_steps(lambda: gm.getrates(P, T, Y, out=W, mode="mixed", stream=stream), steps, 3, stream)
+    gm.getrates(P, T, Y, out=W64, mode="fp64", stream=stream)
+    ms_fused = time_steps(lambda: sur.predict_fused(P, T, Y, W, est), steps, 3, stream)
+    err = ((W - W64).abs().max(dim=0).values / W64.abs().max(dim=0).values).cpu().numpy()
+    run = S.SurrogateGetrates(sur, tol=args.surrogate_tol, exact_mode="mixed")
+    ms_gate = time_steps(lambda: run(P, T, Y), steps, 2, stream)
+    Wg = run(P, T, Y)
+    e_after = ((Wg - W64).abs().max(dim=0).values / W64.abs().max(dim=0).values).cpu().numpy()
+    q = lambda a, v: float(np.quantile(a, v))
+    mp = lambda ms: n / (ms * 1e-3) / 1e6
+    return {"workload": f"53 species / 325 reactions, {n} points (states drawn on the GPU from the workload's "
+                        f"distributions)",
+            "network": "inputs 1000/T, ln T, ln P, 53 ln X (BF16 hi+lo); 3 x 256 GELU; 53 + 2 outputs; "
+                       "BF16 weights, FP32 accumulation",
+            "training": {"samples": info["samples"], "epochs": args.surrogate_epochs, "steps": info["steps"],
+                         "data_s": info["t_data_s"], "train_s": info["t_train_s"],
+                         "error_head_s": info["t_error_head_s"], "final_loss": info["final_loss"]},
+            "err_normwise": {"median": q(err, 0.5), "p90": q(err, 0.9), "p99": q(err, 0.99), "max": float(err.max())},
+            "fused_kernel_mpts": mp(ms_fused), "fp64_kernel_mpts": mp(ms_fp64), "mixed_kernel_mpts": mp(ms_mixed),
+            "gate": {"tol": args.surrogate_tol, "fallback_rate": run.last_fallback,
+                     "mpts_with_fallback": mp(ms_gate),
+                     "err_after_fallback": {"median": q(e_after, 0.5), "p99": q(e_after, 0.99),
+                                            "max": float(e_after.max())}},
+            "gain": {"fused_vs_fp64": ms_fp64 / ms_fused, "fused_vs_mixed": ms_mixed / ms_fused,
+                     "with_fallback_vs_fp64": ms_fp64 / ms_gate, "with_fallback_vs_mixed": ms_mixed / ms_gate}}
+
+
 def time_steps(fn, steps, warmup, stream):
     import torch
     for _ in range(warmup):
@@ -192,7 +269,7 @@ def run_ours(args, rank, world, local_rank):
     blob = pack.pack(mech).to_blob()
     gm = GpuMechanism(mech, device=local_rank, generated=not args.table)
     ng = args.ng
-    P, T, Y = synthetic.states(mech.ns, ng, seed=1000 + rank)
+    P, T, Y = rank_states(mech.ns, ng, rank)
     Pd, Td, Yd = (torch.from_numpy(x).to(dev) for x in (P, T, Y))
     W = torch.empty_like(Yd)
     stream = torch.cuda.current_stream()
@@ -228,13 +305,11 @@ def run_ours(args, rank, world, local_rank):
     results = {}
     for m in modes:
         fn = runner(m)
-        ms = time_steps(fn, args.steps, args.warmup, stream)
         if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            dist.barrier()
+        ms = max_over_ranks(time_steps(fn, args.steps, args.warmup, stream), world, dev)
         kind = gm_tc.kernel_kind("mixed") + "-tensorcore" if m == "mixed_tc" else gm.kernel_kind(m)
-        results[m] = {"ms_per_step": ms, "value": ng * world / (ms * 1e-3) / 1e6, "kernel": kind}
+        results[m] = {"ms_per_step": ms, "value": whole_job_mpts(ng, world, ms), "kernel": kind}
 
     # errors and CPU baseline on a bounded sample (rank 0, single GPU)
     err = {}
@@ -290,14 +365,14 @@ def run_ours(args, rank, world, local_rank):
     t0 = time.perf_counter()
     for _ in range(k_e2e):
         gm_e2e.getrates_host(Ph, Th, Yh, out=Wh.numpy(), mode=mode_e2e)
-    e2e_s = (time.perf_counter() - t0) / max(k_e2e, 1)
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / max(k_e2e, 1), world, dev)
 
     if rank != 0:
         return
+    sur = None
+    if world == 1 and args.surrogate_samples > 0 and mech.ns + 2 <= 64:
+        del Ph, Th, Yh, Wh
+        sur = surrogate_leg(args, gm, stream)
     def roof(m):
         ms = results[m]["ms_per_step"]
         achieved = flop_pt * ng / (ms * 1e-3) / 1e12
@@ -323,7 +398,8 @@ def run_ours(args, rank, world, local_rank):
                     "api": "chemgen_getrates_host (pinned host buffers, 2-stream chunked copies)"},
             "gpu_launches": args.steps,
             "clocks": clocks,
-            "modes": {m: dict(results[m], err=err.get(m), roofline=roof(m)) for m in modes}}
+            "modes": {m: dict(results[m], err=err.get(m), roofline=roof(m)) for m in modes},
+            "surrogate": sur}
     print(json.dumps(line), flush=True)
 
 
