@@ -395,7 +395,7 @@ def run_ours(args, rank, world, local_rank):
             "cpu_baseline": cpu,
             "e2e": {"value": ng * world / e2e_s / 1e6, "unit": "Mpoints/s",
                     "h2d_bytes_per_step": (2 + mech.ns) * ng * 8, "d2h_bytes_per_step": mech.ns * ng * 8,
-                    "api": "chemgen_getrates_host (pinned host buffers, 2-stream chunked copies)"},
+                    "api": "chemgen_getrates_host (pinned host buffers, 3-stream chunked copies)"},
             "gpu_launches": args.steps,
             "clocks": clocks,
             "modes": {m: dict(results[m], err=err.get(m), roofline=roof(m)) for m in modes},

@@ -55,8 +55,9 @@ struct chemgen_handle {
     // host pipeline buffers
     double* iobuf = nullptr;             // device staging of the host-pointer path
     size_t iobuf_doubles = 0;
-    cudaStream_t streams[2] = {nullptr, nullptr};
-    cudaEvent_t ev[2] = {nullptr, nullptr};
+    static constexpr int kIoStreams = 3;
+    cudaStream_t streams[kIoStreams] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev[kIoStreams] = {nullptr, nullptr, nullptr};
     cg::MixedPlan* mixed = nullptr;
     cudaError_t mixed_err = cudaSuccess;
 };
@@ -478,7 +479,7 @@ int chemgen_destroy(chemgen_handle* h) {
     if (h->ws) cudaFree(h->ws);
     if (h->dbuf) cudaFree(h->dbuf);
     if (h->iobuf) cudaFree(h->iobuf);
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < chemgen_handle::kIoStreams; ++i) {
         if (h->streams[i]) cudaStreamDestroy(h->streams[i]);
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);
     }
@@ -578,30 +579,35 @@ int chemgen_getrates_host(chemgen_handle* h, int mode, const double* P, const do
     DeviceGuard g(h->device);
     const int ns = h->ns;
     // chunks of points: each chunk's Y/wdot are [ns][chunk] slices of the
-    // caller's [ns][ng] arrays, copied with one 2D copy each way
-    const int64_t chunk = std::min<int64_t>(ng, std::max<int64_t>(1 << 16, (ng + 3) / 4));
+    // caller's [ns][ng] arrays, copied with one 2D copy each way.  Chunks go
+    // round-robin over three streams, so the host-to-device engine can copy
+    // chunk c+1 and c+2 while chunk c computes and copies back, and a stream is
+    // reused (its in-order queue waiting for chunk c's copy back) only three
+    // chunks later: both copy directions stay busy.
+    constexpr int NS = chemgen_handle::kIoStreams;
+    const int64_t chunk = std::min<int64_t>(ng, std::max<int64_t>(1 << 16, (ng + 15) / 16));
     const size_t per = (size_t)(2 + 2 * ns) * chunk;       // P, T, Y, wdot doubles of one chunk
     std::lock_guard<std::mutex> lk(h->mu);
     cudaError_t e = cudaSuccess;
     if (!h->streams[0]) {
-        for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+        for (int i = 0; i < NS && e == cudaSuccess; ++i) {
             e = cudaStreamCreateWithFlags(&h->streams[i], cudaStreamNonBlocking);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev[i], cudaEventDisableTiming);
         }
         if (e != cudaSuccess) return status_of(e);
     }
-    if (h->iobuf_doubles < 2 * per) {
+    if (h->iobuf_doubles < NS * per) {
         if (h->iobuf) cudaFree(h->iobuf);
         h->iobuf = nullptr;
         h->iobuf_doubles = 0;
-        e = cudaMalloc(&h->iobuf, 2 * per * sizeof(double));
+        e = cudaMalloc(&h->iobuf, NS * per * sizeof(double));
         if (e != cudaSuccess) return status_of(e);
-        h->iobuf_doubles = 2 * per;
+        h->iobuf_doubles = NS * per;
     }
     int status = CHEMGEN_OK;
     int64_t c = 0;
     for (int64_t i0 = 0; i0 < ng && status == CHEMGEN_OK; i0 += chunk, ++c) {
-        const int b = (int)(c & 1);
+        const int b = (int)(c % NS);
         cudaStream_t s = h->streams[b];
         const int64_t n = std::min<int64_t>(chunk, ng - i0);
         double* dP = h->iobuf + (size_t)b * per;
@@ -618,17 +624,16 @@ int chemgen_getrates_host(chemgen_handle* h, int mode, const double* P, const do
             break;
         }
         // the chunk's slices are packed with leading dimension n; chunks in
-        // flight on the two streams share the scratch, so a chunk that needs
-        // scratch waits for the previous chunk's kernel
+        // flight on different streams share the scratch, so a chunk that
+        // needs scratch waits for the previous chunk's kernel
         const size_t need = ws_bytes_for(h, mode, n);
         int st = CHEMGEN_OK;
         if (need) {
             if (need > h->ws_bytes) {
-                cudaStreamSynchronize(h->streams[0]);
-                cudaStreamSynchronize(h->streams[1]);
+                for (int q = 0; q < NS; ++q) cudaStreamSynchronize(h->streams[q]);
                 st = ensure_ws_locked(h, need);
             }
-            if (st == CHEMGEN_OK && c > 0) cudaStreamWaitEvent(s, h->ev[b ^ 1], 0);
+            if (st == CHEMGEN_OK && c > 0) cudaStreamWaitEvent(s, h->ev[(b + NS - 1) % NS], 0);
         }
         if (st == CHEMGEN_OK) st = launch(h, mode, dP, dT, n, dY, dW, h->ws, h->ws_bytes, s);
         if (st) {
@@ -641,10 +646,10 @@ int chemgen_getrates_host(chemgen_handle* h, int mode, const double* P, const do
                                   cudaMemcpyDeviceToHost, s);
         if (e != cudaSuccess) status = status_of(e);
     }
-    cudaError_t e0 = cudaStreamSynchronize(h->streams[0]);
-    cudaError_t e1 = cudaStreamSynchronize(h->streams[1]);
-    if (status == CHEMGEN_OK && e0 != cudaSuccess) status = status_of(e0);
-    if (status == CHEMGEN_OK && e1 != cudaSuccess) status = status_of(e1);
+    for (int q = 0; q < NS; ++q) {
+        const cudaError_t eq = cudaStreamSynchronize(h->streams[q]);
+        if (status == CHEMGEN_OK && eq != cudaSuccess) status = status_of(eq);
+    }
     return status;
 }
 

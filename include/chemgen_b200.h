@@ -78,7 +78,7 @@ int chemgen_getrates_ws(chemgen_handle* h, int mode, const double* P, const doub
 
 /* Host-pointer getrates: copies P, T, Y to the device, computes, copies wdot
  * back, and returns when wdot is on the host.  The copies of one chunk of
- * points overlap the kernels of the previous chunk (two streams).  Pinned
+ * points overlap the kernels and copies of the others (three streams).  Pinned
  * host memory gives the fastest copies; pageable memory works.
  * Replaces: chemgen_m::getrates_gpu (chemgen/templates/chemgen_mod.j2:139-166),
  * which maps host arrays with OpenMP target data. */
