@@ -51,6 +51,7 @@ struct MixedPlan {
     size_t smem = 0;
     int grid = 0;
     int group = 4;          // chunks accumulated in FP32 before the FP64 flush
+    int nt = 1;             // threads per point (blockDim = 128 nt)
     void* dbuf = nullptr;
     const __nv_bfloat16* nu = nullptr;
     int* err = nullptr;
@@ -154,21 +155,13 @@ __device__ double plog_kf64(const DevMech& m, int row, double P, double lnT, dou
     return cgm::cg_exp_clamped(kl + (cgm::cg_log(k[1]) - kl) * (cgm::cg_log(P) - a) / (b - a));
 }
 
-// Net rate of progress of reaction r at this thread's point, FP32.
-__device__ float rate_of_progress(const DevMech& m, int r, const TileCtx& c, int tid) {
-    const DRxn R = load_rxn(m.rxn + r);
-    int kind = CG_STANDARD;
-    while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
-    float Ms = 0.0f;
-    if (kind >= CG_THIRD_BODY && kind <= CG_SRI) {
-        Ms = c.ctot32;
-        for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
-            Ms = fmaf((float)__ldg(m.eff_val + e), c.C[__ldg(m.eff_sp + e) * kTile + tid], Ms);
-    }
+// FP64 evaluation of reaction r (PLOG, non-integer stoichiometry, falloff
+// with negative pre-exponential factors): kept out of line so that the
+// common FP32 path keeps few registers.
+__device__ __noinline__ float rate_of_progress_fp64(const DevMech& m, const DRxn& R, int kind, float Ms,
+                                                    const TileCtx& c, int tid) {
     const bool compact = (R.flags & kFCompact) != 0;
-    const bool neg_falloff = kind >= CG_LINDEMANN && kind <= CG_SRI && (R.flags & (CG_F_A_NEG | CG_F_LOW_NEG));
-    if (!compact || kind == CG_PLOG || neg_falloff) {
-        // FP64 evaluation of this reaction
+    {
         double kf;
         if (kind == CG_PLOG) kf = plog_kf64(m, R.aux, c.Pv, c.lnT, c.invT);
         else if (kind <= CG_THIRD_BODY) kf = R.sgn * cgm::cg_exp_clamped(fma(R.b, c.lnT, R.lnA) - R.theta * c.invT);
@@ -216,6 +209,22 @@ __device__ float rate_of_progress(const DevMech& m, int r, const TileCtx& c, int
         if (kind == CG_THIRD_BODY) rr *= (double)Ms * cs;
         return (float)rr;
     }
+}
+
+// Net rate of progress of reaction r at point `tid` of the tile, FP32.
+__device__ float rate_of_progress(const DevMech& m, int r, const TileCtx& c, int tid) {
+    const DRxn R = load_rxn(m.rxn + r);
+    int kind = CG_STANDARD;
+    while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
+    float Ms = 0.0f;
+    if (kind >= CG_THIRD_BODY && kind <= CG_SRI) {
+        Ms = c.ctot32;
+        for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
+            Ms = fmaf((float)__ldg(m.eff_val + e), c.C[__ldg(m.eff_sp + e) * kTile + tid], Ms);
+    }
+    const bool compact = (R.flags & kFCompact) != 0;
+    const bool neg_falloff = kind >= CG_LINDEMANN && kind <= CG_SRI && (R.flags & (CG_F_A_NEG | CG_F_LOW_NEG));
+    if (!compact || kind == CG_PLOG || neg_falloff) return rate_of_progress_fp64(m, R, kind, Ms, c, tid);
     double a;
     float sgn = 1.0f;
     if (kind <= CG_THIRD_BODY) {
@@ -259,20 +268,27 @@ __device__ float rate_of_progress(const DevMech& m, int r, const TileCtx& c, int
     return sgn * q;
 }
 
-template <bool GS>
-__global__ void __launch_bounds__(kTile, 1)
+// NT threads share each of the tile's 128 points (blockDim = 128 NT): they
+// split the species of the prologue (their partial sums meet in shared
+// memory), the 16 reactions of each chunk, and the accumulator columns of
+// each flush.  The FP32 sums live in tensor memory, so extra threads cost
+// no per-species registers.
+template <bool GS, int NT>
+__global__ void __launch_bounds__(kTile * NT, 1)
     getrates_tc_kernel(DevMech m, const __nv_bfloat16* __restrict__ nu, int npad, int nhalf, int nchunk, uint32_t tcols,
                        const double* __restrict__ P, const double* __restrict__ Tg, const double* __restrict__ Y,
                        double* __restrict__ wdot, int64_t ng, double* __restrict__ gscratch, int* err, int group) {
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int pt = tid & (kTile - 1), sub = tid >> 7;          // point of the tile, share of its work
     const int ns = m.ns;
     unsigned char* sA = sm;                                    // [2 buffers][3 splits][128 x 16] BF16
     unsigned char* sB = sm + 6 * kABytes;                      // [2 buffers][npad x 16] BF16
     float* sC = reinterpret_cast<float*>(sB + 2 * npad * 32);  // [ns][128]
     double* sG = GS ? reinterpret_cast<double*>(sC + ns * kTile) : gscratch + (int64_t)blockIdx.x * ns * kTile;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(sC) + ns * kTile * 4 +
-                                                 (GS ? ns * kTile * 8 : 0));
+    double* sRed = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(sC) + ns * kTile * 4 +
+                                             (GS ? ns * kTile * 8 : 0));   // [NT][128] partial sums
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(sRed + NT * kTile);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
     if (tid == 0) {
         um::mbar_init(&mbar[0], 1);
@@ -291,7 +307,7 @@ __global__ void __launch_bounds__(kTile, 1)
     const int nh = npad / nhalf;
     const int64_t ntiles = (ng + kTile - 1) / kTile;
     for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-        const int64_t i = tile * kTile + tid;
+        const int64_t i = tile * kTile + pt;
         const bool act = i < ng;
         TileCtx c;
         c.C = sC;
@@ -304,25 +320,36 @@ __global__ void __launch_bounds__(kTile, 1)
         c.Tf = (float)c.T;
         c.invTf = (float)c.invT;
         c.lnT2f = (float)c.lnT2;
-        // Y -> C (ytoc.j2), stored as C * 2^32 in FP32
-        double csum = 0.0;
-        for (int k = 0; k < ns; ++k) {
+        // Y -> C (ytoc.j2), stored as C * 2^32 in FP32; species k is handled
+        // by the thread with sub = k % NT
+        double part = 0.0;
+        for (int k = sub; k < ns; k += NT) {
             const double yk = (act ? Y[(int64_t)k * ng + i] : 1.0) * __ldg(m.inv_mw + k);
-            sG[k * kTile + tid] = yk;
-            csum += yk;
+            sG[k * kTile + pt] = yk;
+            part += yk;
         }
+        sRed[sub * kTile + pt] = part;
+        __syncthreads();
+        double csum = 0.0;
+        for (int q = 0; q < NT; ++q) csum += sRed[q * kTile + pt];
         const double facs = c.Pv / (kR0 * csum * c.T) * 4294967296.0;
-        double ctot = 0.0;
-        for (int k = 0; k < ns; ++k) {
-            const double cc = sG[k * kTile + tid] * facs;
-            sC[k * kTile + tid] = (float)cc;
-            ctot += cc;
+        part = 0.0;
+        for (int k = sub; k < ns; k += NT) {
+            const double cc = sG[k * kTile + pt] * facs;
+            sC[k * kTile + pt] = (float)cc;
+            part += cc;
         }
+        __syncthreads();
+        sRed[sub * kTile + pt] = part;
+        __syncthreads();
+        double ctot = 0.0;
+        for (int q = 0; q < NT; ++q) ctot += sRed[q * kTile + pt];
         c.ctot32 = (float)ctot;
         // G = log2(exp(smh) Patm/(R0 T)) (exp_g.j2), FP64
         const double lpfac2 = -6.35856916300311 - c.lnT2;   // log2(Patm/R0) - log2 T
-        for (int k = 0; k < ns; ++k)
-            sG[k * kTile + tid] = fma(species_smh(m.thermo, k, c.T, c.lnT, c.invT), kLog2eD, lpfac2);
+        for (int k = sub; k < ns; k += NT)
+            sG[k * kTile + pt] = fma(species_smh(m.thermo, k, c.T, c.lnT, c.invT), kLog2eD, lpfac2);
+        __syncthreads();
         bool first_group = true;
         for (int ch = 0; ch < nchunk && ok; ++ch) {
             const int buf = ch & 1;
@@ -335,18 +362,18 @@ __global__ void __launch_bounds__(kTile, 1)
             // the chunk's stoichiometry, B operand [npad x 16], canonical layout
             const uint4* src = reinterpret_cast<const uint4*>(nu + (int64_t)ch * npad * kChunk);
             uint4* dst = reinterpret_cast<uint4*>(sB + buf * npad * 32);
-            for (int q = tid; q < npad * 2; q += kTile) dst[q] = __ldg(src + q);
+            for (int q = tid; q < npad * 2; q += kTile * NT) dst[q] = __ldg(src + q);
             // q for the chunk's reactions -> A operands (hi, mid, lo)
             unsigned char* a0 = sA + buf * 3 * kABytes;
-            for (int j = 0; j < kChunk; ++j) {
+            for (int j = sub; j < kChunk; j += NT) {
                 const int r = ch * kChunk + j;
-                float q = (r < m.nr) ? rate_of_progress(m, r, c, tid) : 0.0f;
+                float q = (r < m.nr) ? rate_of_progress(m, r, c, pt) : 0.0f;
                 if (!act) q = 0.0f;
                 const __nv_bfloat16 h = __float2bfloat16_rn(q);
                 const float r1 = q - __bfloat162float(h);
                 const __nv_bfloat16 md = __float2bfloat16_rn(r1);
                 const __nv_bfloat16 lo = __float2bfloat16_rn(r1 - __bfloat162float(md));
-                const uint32_t off = um::kmajor_offset(tid, j, kChunk);
+                const uint32_t off = um::kmajor_offset(pt, j, kChunk);
                 *reinterpret_cast<__nv_bfloat16*>(a0 + off) = h;
                 *reinterpret_cast<__nv_bfloat16*>(a0 + kABytes + off) = md;
                 *reinterpret_cast<__nv_bfloat16*>(a0 + 2 * kABytes + off) = lo;
@@ -370,7 +397,8 @@ __global__ void __launch_bounds__(kTile, 1)
             pending[buf] = true;
             if ((ch % group) == group - 1 || ch == nchunk - 1) {
                 // end of a group of reactions: wait for its MMAs, then add the
-                // FP32 partial sums into the FP64 output
+                // FP32 partial sums into the FP64 output; the NT warps that
+                // share a lane quadrant split the columns
                 for (int b = 0; b < 2; ++b)
                     if (pending[b]) {
                         ok = um::mbar_wait(&mbar[b], parity[b]) && ok;
@@ -379,9 +407,9 @@ __global__ void __launch_bounds__(kTile, 1)
                     }
                 um::fence_after_sync();
                 if (ok) {
-                    for (int col = 0; col < npad; col += 16) {
+                    for (int col = 16 * (warp >> 2); col < npad; col += 16 * NT) {
                         float v[16];
-                        um::tmem_ld16(um::tmem_lane_addr(tbase, warp, col), v);
+                        um::tmem_ld16(um::tmem_lane_addr(tbase, warp & 3, col), v);
                         if (act)
                             for (int j = 0; j < 16; ++j)
                                 if (col + j < ns) {
@@ -403,6 +431,22 @@ __global__ void __launch_bounds__(kTile, 1)
     if (warp == 0) um::tmem_dealloc(tbase, tcols);
 }
 
+const void* kernel_for(int g_smem, int nt) {
+    if (g_smem) return nt == 4 ? (const void*)getrates_tc_kernel<true, 4>
+                               : nt == 2 ? (const void*)getrates_tc_kernel<true, 2> : (const void*)getrates_tc_kernel<true, 1>;
+    return nt == 4 ? (const void*)getrates_tc_kernel<false, 4>
+                   : nt == 2 ? (const void*)getrates_tc_kernel<false, 2> : (const void*)getrates_tc_kernel<false, 1>;
+}
+
+template <bool GS, int NT>
+cudaError_t launch_tc(const MixedPlan* p, const DevMech& m, const double* P, const double* T, const double* Y,
+                      double* wdot, int64_t ng, double* scratch, int64_t grid, cudaStream_t s) {
+    getrates_tc_kernel<GS, NT><<<(unsigned)grid, kTile * NT, p->smem, s>>>(m, p->nu, p->npad, p->nhalf, p->nchunk,
+                                                                           p->tcols, P, T, Y, wdot, ng, scratch,
+                                                                           p->err, p->group);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- host side
@@ -415,7 +459,8 @@ cudaError_t mixed_prepare(const DevMech& m, const cg_mech_view& v, int device, M
     uint32_t tcols = 32;
     while ((int)tcols < npad) tcols <<= 1;
     const int nchunk = (nr + kChunk - 1) / kChunk;
-    const size_t base = 6 * (size_t)kABytes + 2 * (size_t)npad * 32 + (size_t)ns * kTile * 4 + 32;
+    // the largest share count is planned for; the [nt][128] partial-sum slots follow the state
+    const size_t base = 6 * (size_t)kABytes + 2 * (size_t)npad * 32 + (size_t)ns * kTile * 4 + 4 * kTile * 8 + 32;
     const size_t with_g = base + (size_t)ns * kTile * 8;
     cudaDeviceProp prop;
     cudaError_t e = cudaGetDeviceProperties(&prop, device);
@@ -439,6 +484,18 @@ cudaError_t mixed_prepare(const DevMech& m, const cg_mech_view& v, int device, M
     int per_sm = (int)(prop.sharedMemPerMultiprocessor / (p->smem + 1024));
     per_sm = std::min(per_sm, (int)(512 / tcols));
     per_sm = std::max(per_sm, 1);
+    // threads per point: the most (4, 2, 1) whose registers still let per_sm
+    // CTAs share the SM's register file
+    p->nt = 1;
+    for (int nt : {4, 2}) {
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, kernel_for(p->g_smem, nt)) != cudaSuccess) continue;
+        if ((long)per_sm * kTile * nt * fa.numRegs <= prop.regsPerMultiprocessor &&
+            per_sm * kTile * nt <= prop.maxThreadsPerMultiProcessor) {
+            p->nt = nt;
+            break;
+        }
+    }
     p->grid = prop.multiProcessorCount * per_sm;
     // nu chunks in the canonical K-major layout: B[n][k] = nu of species n in reaction 16*chunk + k
     std::vector<float> nuf((size_t)ns * nr, 0.0f);
@@ -473,11 +530,8 @@ cudaError_t mixed_prepare(const DevMech& m, const cg_mech_view& v, int device, M
     e = cudaMalloc(&p->dbuf, bytes);
     if (e == cudaSuccess) e = cudaMemcpy(p->dbuf, img.data(), img.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset((char*)p->dbuf + bytes - 256, 0, 256);
-    if (e == cudaSuccess) {
-        auto k64 = getrates_tc_kernel<true>;
-        auto k32 = getrates_tc_kernel<false>;
-        e = cudaFuncSetAttribute(p->g_smem ? k64 : k32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem);
-    }
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kernel_for(p->g_smem, p->nt),
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem);
     if (e != cudaSuccess) {
         if (p->dbuf) cudaFree(p->dbuf);
         delete p;
@@ -513,14 +567,15 @@ cudaError_t launch_getrates_mixed(const MixedPlan* p, const DevMech& m, const do
         grid = std::min<int64_t>(grid, fit);
         if (grid < 1 || !scratch) return cudaErrorInvalidValue;
     }
-    if (p->g_smem)
-        getrates_tc_kernel<true><<<(unsigned)grid, kTile, p->smem, s>>>(m, p->nu, p->npad, p->nhalf, p->nchunk, p->tcols,
-                                                                        P, T, Y, wdot, ng, nullptr, p->err, p->group);
-    else
-        getrates_tc_kernel<false><<<(unsigned)grid, kTile, p->smem, s>>>(m, p->nu, p->npad, p->nhalf, p->nchunk,
-                                                                         p->tcols, P, T, Y, wdot, ng, (double*)scratch,
-                                                                         p->err, p->group);
-    return cudaGetLastError();
+    double* gs = p->g_smem ? nullptr : (double*)scratch;
+    switch ((p->g_smem ? 10 : 0) + p->nt) {
+        case 14: return launch_tc<true, 4>(p, m, P, T, Y, wdot, ng, gs, grid, s);
+        case 12: return launch_tc<true, 2>(p, m, P, T, Y, wdot, ng, gs, grid, s);
+        case 11: return launch_tc<true, 1>(p, m, P, T, Y, wdot, ng, gs, grid, s);
+        case 4: return launch_tc<false, 4>(p, m, P, T, Y, wdot, ng, gs, grid, s);
+        case 2: return launch_tc<false, 2>(p, m, P, T, Y, wdot, ng, gs, grid, s);
+        default: return launch_tc<false, 1>(p, m, P, T, Y, wdot, ng, gs, grid, s);
+    }
 }
 
 int mixed_error_flag(const MixedPlan* p) {
