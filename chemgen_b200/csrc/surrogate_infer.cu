@@ -261,16 +261,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (l < 3) {
                     const float* bl = sBias + kHid * l;
 #pragma unroll 1
-                    for (int c = 128 * ehalf; c < 128 * ehalf + 128; c += 32) {
-                        uint32_t ra[16], rb[16];
-                        um::tmem_ld16_nowait(um::tmem_lane_addr(tbase, g4, c), ra);
-                        um::tmem_ld16_nowait(um::tmem_lane_addr(tbase, g4, c + 16), rb);
-                        um::tmem_wait_ld(ra);
-                        um::tmem_wait_ld(rb);
-                        gelu_store16(ra, bl + c, sA + um::kmajor_offset(erow, c, kHid),
-                                     sA + um::kmajor_offset(erow, c + 8, kHid));
-                        gelu_store16(rb, bl + c + 16, sA + um::kmajor_offset(erow, c + 16, kHid),
-                                     sA + um::kmajor_offset(erow, c + 24, kHid));
+                    for (int c = 128 * ehalf; c < 128 * ehalf + 128; c += 64) {
+                        // one 64-column load, then 64 independent GELUs
+                        uint32_t r[64];
+                        um::tmem_ld64(um::tmem_lane_addr(tbase, g4, c), r);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            gelu_store16(r + 16 * q, bl + c + 16 * q, sA + um::kmajor_offset(erow, c + 16 * q, kHid),
+                                         sA + um::kmajor_offset(erow, c + 16 * q + 8, kHid));
                     }
                 } else {
                     const float* b4 = sBias + 3 * kHid;
