@@ -62,13 +62,23 @@ __device__ __forceinline__ double f32_scaled_to_f64(float v, int k) {
     return e == 0 ? 0.0 : (e == 2047 ? __longlong_as_double(0x7ff0000000000000LL | ((long long)(b & 0x80000000u) << 32)) : r);
 }
 
+// 2^k as FP64 for an integer k, built in the exponent field; k is clamped
+// to [-1023, 1023] (2^-1023 encodes as +0).
+__device__ __forceinline__ double exp2i(int k) {
+    const int e = max(0, min(k + 1023, 2046));
+    return __hiloint2double(e << 20, 0);
+}
+
 // q = 2^a * prod  (prod an FP32 product of scaled concentrations, eoff the
-// integer exponent that undoes their scaling).
+// integer exponent that undoes their scaling): the FP32 value 2^f * prod,
+// converted exactly to FP64, times 2^(n + eoff).  For results in the FP64
+// normal range this is bit-identical to rebuilding the double from the
+// float's fields (f32_scaled_to_f64), in fewer instructions.
 __device__ __forceinline__ double rate2(double a, float prod, int eoff) {
     int n;
     float f;
     split2(a, n, f);
-    return f32_scaled_to_f64(ex2f(f) * prod, n + eoff);
+    return (double)(ex2f(f) * prod) * exp2i(n + eoff);
 }
 
 }  // namespace cgg

@@ -531,9 +531,22 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 GEN_DIR = os.path.join(HERE, "_generated")
 
 
+def codegen_version() -> str:
+    """Short hash of this emitter and the headers generated code includes, so
+    that a change to either gives built modules a new name (and a rebuild)."""
+    h = hashlib.sha256()
+    files = [os.path.abspath(__file__)] + [os.path.join(HERE, "csrc", f) for f in
+                                           ("gen_common.cuh", "cg_math.cuh")]
+    files.append(os.path.join(os.path.dirname(HERE), "include", "chemgen_b200.h"))
+    for f in files:
+        with open(f, "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:8]
+
+
 def module_path(mech: Mechanism) -> str:
     fp = fingerprint(pack(mech).to_blob())
-    return os.path.join(GEN_DIR, f"libcg_{fp:016x}.so")
+    return os.path.join(GEN_DIR, f"libcg_{fp:016x}_{codegen_version()}.so")
 
 
 def build_module(mech: Mechanism, out: Optional[str] = None, verbose: bool = False, keep_source: bool = True,
