@@ -69,6 +69,28 @@ __device__ __forceinline__ double exp2i(int k) {
     return __hiloint2double(e << 20, 0);
 }
 
+// 2^k as FP32 for -126 <= k <= 127, built in the exponent field (unsigned
+// shift: no signed-overflow arithmetic for any k).
+__device__ __forceinline__ float exp2f_int(int k) { return __uint_as_float((unsigned int)(k + 127) << 23); }
+
+// lg2 of Pr/(1+Pr) for Pr = mpr 2^npr (mpr in [0.5, 1), l2m = lg2 mpr):
+// Pr < 1: npr + l2m - lg2(1 + Pr), reported as l2r = l2m - lg2(1 + Pr) with
+// nfix = npr; Pr >= 1: l2r = -lg2(1 + 1/Pr), nfix = 0.  Terms below 2^-126
+// are dropped.  (A branch-free select of the two forms gave wrong results
+// inside the large generated kernels although it matched this form in a
+// stand-alone test; the branch is kept.)
+__device__ __forceinline__ void falloff_blend(float mpr, int npr, float l2m, float& l2r, int& nfix) {
+    if (npr < 0) {
+        const float pr = npr > -126 ? mpr * exp2f_int(npr) : 0.0f;
+        l2r = l2m - lg2f(1.0f + pr);
+        nfix = npr;
+    } else {
+        const float ipr = npr < 126 ? __fdividef(1.0f, mpr) * exp2f_int(-npr) : 0.0f;
+        l2r = -lg2f(1.0f + ipr);
+        nfix = 0;
+    }
+}
+
 // q = 2^a * prod  (prod an FP32 product of scaled concentrations, eoff the
 // integer exponent that undoes their scaling): the FP32 value 2^f * prod,
 // converted exactly to FP64, times 2^(n + eoff).  For results in the FP64

@@ -100,17 +100,11 @@ __device__ double falloff_l2(int kind, int flags, const DRxn& R, const DFall& f,
     const int ex = ((__float_as_int(mpr) >> 23) & 0xff) - 126;
     npr += ex - 32;
     mpr = __int_as_float((__float_as_int(mpr) & 0x807fffff) | (126 << 23));   // [0.5, 1)
-    const float l2pr = (float)npr + cgg::lg2f(mpr);
+    const float l2m = cgg::lg2f(mpr);
+    const float l2pr = (float)npr + l2m;
     float l2r;
-    int nfix = 0;
-    if (npr < 0) {
-        const float pr = npr > -126 ? ldexpf(mpr, npr) : 0.0f;
-        l2r = cgg::lg2f(mpr) - cgg::lg2f(1.0f + pr);
-        nfix = npr;
-    } else {
-        const float ipr = npr < 126 ? ldexpf(1.0f / mpr, -npr) : 0.0f;
-        l2r = -cgg::lg2f(1.0f + ipr);
-    }
+    int nfix;
+    cgg::falloff_blend(mpr, npr, l2m, l2r, nfix);
     float l2F = 0.0f;
     if (kind == CG_TROE) {
         float Fc = fmaf((float)f.p[0], cgg::ex2f(-kLog2eF * c.Tf * (float)f.p[1]),

@@ -281,11 +281,9 @@ class _Emitter:
         L.append("float mpr = cgg::ex2f(fpr) * Ms;")
         L.append("int ex = ((__float_as_int(mpr) >> 23) & 0xff) - 126; npr += ex - 32;")
         L.append("mpr = __int_as_float((__float_as_int(mpr) & 0x807fffff) | (126 << 23));   // [0.5, 1)")
-        # lg2 Pr/(1+Pr) = npr + lg2(mpr) - lg2(1+Pr) (Pr < 1) or -lg2(1+1/Pr)
-        L.append("float l2r; int nfix = 0; const float l2pr = (float)npr + cgg::lg2f(mpr);")
-        L.append("if (npr < 0) { const float pr = npr > -126 ? ldexpf(mpr, npr) : 0.0f; "
-                 "l2r = cgg::lg2f(mpr) - cgg::lg2f(1.0f + pr); nfix = npr; }")
-        L.append("else { const float ipr = npr < 126 ? ldexpf(1.0f / mpr, -npr) : 0.0f; l2r = -cgg::lg2f(1.0f + ipr); }")
+        # lg2 Pr/(1+Pr) = npr + lg2(mpr) - lg2(1+Pr) (Pr < 1) or -lg2(1+1/Pr), branch-free
+        L.append("float l2r; int nfix; const float l2m = cgg::lg2f(mpr); const float l2pr = (float)npr + l2m;")
+        L.append("cgg::falloff_blend(mpr, npr, l2m, l2r, nfix);")
         if r.kind == "troe":
             a, T3, T1 = (r15(x) for x in r.troe[:3])
             fc = (f"fmaf({_f(r15(1.0 - a))}, cgg::ex2f({_f(-LOG2E / T3)}*Tf), "
