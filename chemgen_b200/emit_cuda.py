@@ -32,7 +32,7 @@ LOG10_2 = 0.30102999566398119521
 CSCALE_LOG2 = 32          # mixed: concentrations are stored as C * 2^32 in FP32
 # register-resident wdot accumulators up to this many species
 MAX_REG_SPECIES = 72
-SYNC_EVERY = 8            # reactions between block barriers
+SYNC_EVERY = 48           # reactions between block barriers (B200 sweep at 53/325: 2..64, best 48-64)
 SMEM_BUDGET = 220 * 1024  # dynamic shared memory per block
 
 
@@ -59,7 +59,7 @@ def _f(x: float) -> str:
 
 
 class _Emitter:
-    def __init__(self, mech: Mechanism, block: int, sync_every: int = 8):
+    def __init__(self, mech: Mechanism, block: int, sync_every: int = SYNC_EVERY):
         self.sync_every = sync_every
         self.mech = mech
         self.ns = mech.ns
