@@ -56,11 +56,16 @@ __device__ __forceinline__ double cg_rcp(double x) {
     return fma(r, e, r);
 }
 
+// Non-positive, infinite, NaN and subnormal arguments: the library log, kept
+// out of line so that the straight-line generated kernels do not carry a copy
+// of it at every call site.
+static __device__ __noinline__ double cg_log_special(double x) { return log(x); }
+
 __device__ __forceinline__ double cg_log(double x) {
     const int hi = __double2hiint(x);
     const int lo = __double2loint(x);
     // normal, finite, positive: biased exponent in [1, 2046], sign clear
-    if (hi < 0x00100000 || hi >= 0x7ff00000) return log(x);
+    if (hi < 0x00100000 || hi >= 0x7ff00000) return cg_log_special(x);
     int e = (hi >> 20) - 1023;
     int mh = (hi & 0x000fffff) | 0x3ff00000;          // m in [1, 2)
     if (mh > 0x3ff6a09e) {                            // m > sqrt(2): use m/2
