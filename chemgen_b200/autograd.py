@@ -15,19 +15,31 @@ class Getrates(torch.autograd.Function):
     """wdot = getrates(P, T, Y) with an analytic backward."""
 
     @staticmethod
-    def forward(ctx, gm: GpuMechanism, P, T, Y, mode: str = "fp64"):
-        P, T, Y = P.contiguous(), T.contiguous(), Y.contiguous()
+    def forward(ctx, gm: GpuMechanism, P, T, Y, mode: str = "fp64", layout: str = "species_major"):
+        if layout not in ("species_major", "point_major"):
+            raise ValueError("layout must be 'species_major' or 'point_major'")
+        P, T = P.contiguous(), T.contiguous()
+        Ys = Y.t().contiguous() if layout == "point_major" else Y.contiguous()
         ctx.gm = gm
-        ctx.save_for_backward(P, T, Y)
-        return gm.getrates(P, T, Y, mode=mode)
+        ctx.layout = layout
+        ctx.save_for_backward(P, T, Ys)
+        w = gm.getrates(P, T, Ys, mode=mode)
+        return w.t().contiguous() if layout == "point_major" else w
 
     @staticmethod
     def backward(ctx, g):
-        P, T, Y = ctx.saved_tensors
-        gT, gY, gP = ctx.gm.vjp(P, T, Y, g.contiguous())
-        return None, gP, gT, gY, None
+        P, T, Ys = ctx.saved_tensors
+        gs = g.t().contiguous() if ctx.layout == "point_major" else g.contiguous()
+        gT, gY, gP = ctx.gm.vjp(P, T, Ys, gs)
+        if ctx.layout == "point_major":
+            gY = gY.t().contiguous()
+        return None, gP, gT, gY, None, None
 
 
-def getrates(gm: GpuMechanism, P, T, Y, mode: str = "fp64"):
-    """Differentiable getrates on CUDA float64 tensors (Y is [ns, ng])."""
-    return Getrates.apply(gm, P, T, Y, mode)
+GetratesFn = Getrates
+
+
+def getrates(gm: GpuMechanism, P, T, Y, mode: str = "fp64", layout: str = "species_major"):
+    """Differentiable getrates on CUDA float64 tensors: Y [ns, ng] (or
+    [ng, ns] with layout="point_major"), wdot in the same layout."""
+    return Getrates.apply(gm, P, T, Y, mode, layout)

@@ -197,9 +197,24 @@ class GpuMechanism:
         check(lib().chemgen_getrates_ex(self._h, MODES[mode], P, T, ng, Y, wdot, _stream(stream)),
               "chemgen_getrates_ex")
 
-    def getrates(self, P, T, Y, out=None, mode: str = "fp64", stream=None):
-        """torch CUDA float64 tensors: P[ng], T[ng], Y[ns, ng] -> wdot[ns, ng]."""
+    def getrates(self, P, T, Y, out=None, mode: str = "fp64", stream=None, layout: str = "species_major"):
+        """torch CUDA float64 tensors: P[ng], T[ng], Y[ns, ng] -> wdot[ns, ng].
+
+        layout="point_major" takes Y as [ng, ns] (per point, species
+        contiguous: the reference's Python getrates_i layout) and returns wdot
+        the same way; the kernels run on a species-major copy."""
         import torch
+        if layout not in ("species_major", "point_major"):
+            raise ValueError("layout must be 'species_major' or 'point_major'")
+        if layout == "point_major":
+            if Y.dim() != 2 or Y.shape[1] != self.ns:
+                raise ValueError(f"point-major Y must be [ng, {self.ns}]")
+            w = self.getrates(P, T, Y.t().contiguous(), mode=mode, stream=stream)
+            w = w.t()
+            if out is not None:
+                out.copy_(w)
+                return out
+            return w.contiguous()
         ns, ng = Y.shape
         if ns != self.ns:
             raise ValueError(f"Y has {ns} species, the mechanism {self.ns}")
