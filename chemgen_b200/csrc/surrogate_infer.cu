@@ -2,25 +2,29 @@
 // features -> 4 MLP layers -> decoded FP64 wdot in one kernel, activations
 // never leaving the SM.
 //
-// One persistent CTA of 256 threads per SM works through tiles of 128 points:
-// * features: each point's 64 network inputs (1000/T, ln T, ln P/1 atm,
-//   ln X_k, zeros), centred and scaled, split into BF16 hi + lo parts, are
-//   written straight into the shared-memory A operand [128 x 128] in the
-//   K-major canonical layout;
-// * layer l: one thread issues K/16 tcgen05.mma (M = 128, N = 256 or 64,
-//   K = 16, BF16 in, FP32 accumulate in tensor memory) against the layer's
-//   weights, which a bulk asynchronous copy (cp.async.bulk, no multicast)
-//   brought into shared memory while the previous epilogue ran;
-// * epilogue l < 3: tcgen05.ld of the accumulators, bias, GELU (tanh form,
-//   hardware tanh as in training), BF16, back into the A operand of the next
-//   layer (K = 256);
-// * epilogue l = 3: w_k = (u_k + b_k) exp(c + s (L + b_L)) in FP64, stored
-//   species-major, and the error estimate.
+// One persistent CTA of 384 threads per SM works through tiles of 128 points,
+// in two warp groups that run one tile apart:
+// * feature group (warps 8-11, one thread per point): the next tile's 64
+//   network inputs (1000/T, ln T, ln P/1 atm, ln X_k, zeros), centred and
+//   scaled, split into BF16 hi + lo parts, written into their own
+//   shared-memory A operand [128 x 128] (K-major canonical layout); then 128
+//   arrivals on the "features full" mbarrier.  It writes tile j+1 only after
+//   the first layer of tile j has consumed tile j ("features empty");
+// * compute group (warps 0-7): per layer one thread issues K/16 tcgen05.mma
+//   (M = 128, N = 256 or 64, K = 16, BF16 in, FP32 accumulate in tensor
+//   memory) against the layer's weights, which a bulk asynchronous copy
+//   (cp.async.bulk, no multicast) brought into shared memory while the
+//   previous epilogue ran; epilogue l < 3: tcgen05.ld, bias, GELU (tanh form,
+//   hardware tanh as in training), BF16, into the A operand of the next layer
+//   (K = 256); epilogue l = 3: w_k = (u_k + b_k) exp(c + s (L + b_L)) in FP64,
+//   stored species-major, and the error estimate.  The compute group
+//   synchronises on its own named barrier.
 // The weights come pre-arranged in the canonical layout (chemgen_surrogate_pack),
 // so every weight load is a straight 16-byte-aligned bulk copy.  Shared
-// memory: 64 KB activations + 128 KB weights; tensor memory: 256 columns.
-// Every mbarrier wait is bounded; a time-out sets the error word and the
-// kernel drains what it issued before freeing tensor memory.
+// memory: 64 KB activations + 32 KB features + 128 KB weights; tensor memory:
+// 256 columns; biases are read through the read-only cache.  Every mbarrier
+// wait is bounded; a time-out sets the error word and the kernel drains what
+// it issued before freeing tensor memory.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -34,17 +38,15 @@ namespace {
 
 using bf16 = __nv_bfloat16;
 
-constexpr int kPts = 128, kThreads = 256;
+constexpr int kPts = 128, kCompute = 256, kThreads = kCompute + kPts;
 constexpr int kDin = 64, kK1 = 2 * kDin, kHid = 256, kDout = 64;
 constexpr int kW1 = kHid * kK1, kW2 = kHid * kHid, kW4 = kDout * kHid;
 constexpr int kImgElems = kW1 + 2 * kW2 + kW4;
-constexpr int kBiasElems = 3 * kHid + kDout;
-constexpr uint32_t kABytes = kPts * kHid * 2;
+constexpr uint32_t kABytes = kPts * kHid * 2;                // hidden activations, K = 256
+constexpr uint32_t kFBytes = kPts * kK1 * 2;                 // features, K = 128
 constexpr uint32_t kWBytes = kHid * kHid * 2;
-constexpr uint32_t kTailOff = kABytes + kWBytes;            // barriers, flags, TMEM slot (64 B)
-constexpr uint32_t kPartOff = kTailOff + 64;                 // [2][128] partial mixture sums
-constexpr uint32_t kBiasOff = kPartOff + 2 * kPts * 4;       // [832] biases
-constexpr size_t kSmem = (size_t)kBiasOff + kBiasElems * 4;
+constexpr uint32_t kFOff = kABytes, kWOff = kFOff + kFBytes, kTailOff = kWOff + kWBytes;
+constexpr size_t kSmem = (size_t)kTailOff + 64;             // 4 mbarriers, TMEM slot, flags
 constexpr uint32_t kCopyPiece = 16384;
 
 __device__ int g_sur_err;
@@ -69,12 +71,13 @@ __device__ __forceinline__ float gelu_fast(float z) {
     return fmaf(hz, t, hz);
 }
 
-__device__ __forceinline__ void gelu_store16(const uint32_t* r, const float* b, unsigned char* dst0,
+// 16 accumulators + bias -> GELU -> BF16, two 16-byte stores (8 columns each).
+__device__ __forceinline__ void gelu_store16(const uint32_t* r, const float* __restrict__ b, unsigned char* dst0,
                                              unsigned char* dst1) {
     uint32_t pk[8];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        const float4 bb = *reinterpret_cast<const float4*>(b + 4 * q);
+        const float4 bb = __ldg(reinterpret_cast<const float4*>(b) + q);
         const float z0 = __uint_as_float(r[4 * q]) + bb.x, z1 = __uint_as_float(r[4 * q + 1]) + bb.y;
         const float z2 = __uint_as_float(r[4 * q + 2]) + bb.z, z3 = __uint_as_float(r[4 * q + 3]) + bb.w;
         pk[2 * q] = pack2(__float2bfloat16(gelu_fast(z0)), __float2bfloat16(gelu_fast(z1)));
@@ -91,6 +94,62 @@ __device__ __forceinline__ void issue_weights(const bf16* img, int l, unsigned c
     for (uint32_t o = 0; o < bytes; o += kCopyPiece) um::bulk_g2s(sW + o, src + o, kCopyPiece, wbar);
 }
 
+// Feature group: the 64 inputs of point `row` of `tile`, as BF16 hi/lo parts
+// into sF (K = 128 canonical layout).  All loads use clamped (valid) indices
+// so that they are in flight together; absent points and padding give 0.
+__device__ __forceinline__ void write_features(unsigned char* sF, int row, int64_t tile, int64_t ng, int ns,
+                                               const double* __restrict__ P, const double* __restrict__ T,
+                                               const double* __restrict__ Y, const double* __restrict__ inv_mw,
+                                               const float* nrm) {
+    const int64_t i = tile * kPts + row;
+    const bool act = i < ng;
+    const int64_t ic = act ? i : ng - 1;
+    float y[kDin - 3];
+#pragma unroll
+    for (int k = 0; k < kDin - 3; ++k) y[k] = (float)__ldg(Y + (int64_t)min(k, ns - 1) * ng + ic);
+    const double t = __ldg(T + ic);
+    const float invT = (float)(1000.0 / t), lnT = logf((float)t), lnP = logf((float)(__ldg(P + ic) / 1013250.0));
+    float mix = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kDin - 3; ++k)
+        if (k < ns) mix = fmaf(fmaxf(y[k], 0.0f), (float)__ldg(inv_mw + k), mix);
+    const float lmix = __logf(fmaxf(mix, 1e-37f));
+#pragma unroll
+    for (int g = 0; g < kDin / 8; ++g) {
+        uint32_t hi[4], lo[4];
+#pragma unroll
+        for (int u = 0; u < 8; u += 2) {
+            float f[2];
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int j = 8 * g + u + e, k = j - 3;
+                float v = 0.0f;
+                if (act) {
+                    if (j == 0) {
+                        v = (invT - nrm[0]) * nrm[1];
+                    } else if (j == 1) {
+                        v = (lnT - nrm[2]) * nrm[3];
+                    } else if (j == 2) {
+                        v = (lnP - nrm[4]) * nrm[5];
+                    } else if (k < ns) {
+                        // fast log: ~1e-5 absolute, below the ~2^-16 of the split inputs
+                        const float lx = __logf(fmaxf(y[k], 1e-30f) * (float)__ldg(inv_mw + k)) - lmix;
+                        v = fminf(fmaxf((lx - nrm[6]) * nrm[7], -6.0f), 6.0f);
+                    }
+                }
+                f[e] = v;
+            }
+            const bf16 h0 = __float2bfloat16(f[0]), h1 = __float2bfloat16(f[1]);
+            hi[u / 2] = pack2(h0, h1);
+            lo[u / 2] = pack2(__float2bfloat16(f[0] - __bfloat162float(h0)),
+                              __float2bfloat16(f[1] - __bfloat162float(h1)));
+        }
+        *reinterpret_cast<uint4*>(sF + um::kmajor_offset(row, 8 * g, kK1)) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<uint4*>(sF + um::kmajor_offset(row, kDin + 8 * g, kK1)) =
+            make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    }
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
     surrogate_infer_kernel(const bf16* __restrict__ img, const float* __restrict__ bias,
                            const float* __restrict__ norm, const float* __restrict__ lnorm,
@@ -99,23 +158,26 @@ __global__ void __launch_bounds__(kThreads, 1)
                            double* __restrict__ W, float* __restrict__ est) {
     extern __shared__ __align__(1024) unsigned char sm[];
     unsigned char* sA = sm;
-    unsigned char* sW = sm + kABytes;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kTailOff);          // [0] MMAs done, [1] weights landed
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
-    volatile int* wfail = reinterpret_cast<volatile int*>(bars + 3);       // set by thread 0 before a barrier
-    volatile int* mfail = wfail + 1;                                        // set after the MMA wait
-    float* sPart = reinterpret_cast<float*>(sm + kPartOff);
-    float* sBias = reinterpret_cast<float*>(sm + kBiasOff);
+    unsigned char* sF = sm + kFOff;
+    unsigned char* sW = sm + kWOff;
+    // [0] MMAs done, [1] weights landed, [2] features full (128 arrivals), [3] features empty
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kTailOff);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 4);
+    volatile int* wfail = reinterpret_cast<volatile int*>(tslot + 1);   // set by thread 0 before a barrier
+    volatile int* mfail = wfail + 1;                                     // set after the MMA wait
+    volatile int* ffail = wfail + 2;                                     // feature group gave up
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int64_t ntiles = (ng + kPts - 1) / kPts;
     if (tid == 0) {
         um::mbar_init(&bars[0], 1);
         um::mbar_init(&bars[1], 1);
+        um::mbar_init(&bars[2], kPts);
+        um::mbar_init(&bars[3], 1);
         *wfail = 0;
         *mfail = 0;
+        *ffail = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int q = tid; q < kBiasElems; q += kThreads) sBias[q] = __ldg(bias + q);
     if (warp == 0) um::tmem_alloc(tslot, 256);
     um::fence_before_sync();
     __syncthreads();
@@ -124,196 +186,145 @@ __global__ void __launch_bounds__(kThreads, 1)
     float nrm[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) nrm[q] = __ldg(norm + q);
-    const double lc = (double)__ldg(lnorm), ls = (double)__ldg(lnorm + 1);
+    bool failed = false, w_pending = false, m_failed = false;
     uint32_t mpar = 0, wpar = 0;
-    bool w_pending = false, m_failed = false;
-    if (tid == 0) {
-        issue_weights(img, 0, sW, &bars[1]);
-        w_pending = true;
-    }
-    const int row = tid & (kPts - 1), half = tid >> 7;  // features: point, which 32 inputs
-    const int g4 = warp & 3, ehalf = warp >> 2;         // epilogue: TMEM lane group, column half
-    const int erow = 32 * g4 + lane;
-    bool failed = false;
-    for (int64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-        // the next tile's inputs start moving into L2 now
-        if (warp == 7 && tile + gridDim.x < ntiles) {
-            const int64_t n0 = (tile + gridDim.x) * kPts;
-            const uint32_t bytes = (uint32_t)(min((int64_t)kPts, ng - n0) * 8) & ~15u;
-            for (int r = lane; r < ns + 2 && bytes; r += 32) {
-                const double* src = r < ns ? Y + (int64_t)r * ng + n0 : (r == ns ? T + n0 : P + n0);
-                if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) um::bulk_prefetch_l2(src, bytes);
-            }
-        }
-        // ---- features -> A [128 x 128].  Thread (row, half) owns inputs
-        // 32 half .. 32 half + 31 of point `row`: it loads all of its mass
-        // fractions at once, and the two halves add their parts of
-        // sum_k Y_k / W_k through shared memory.
-        {
-            const int64_t i = tile * kPts + row;
-            const bool act = i < ng;
-            const int jb = 32 * half;
-            // unconditional loads from clamped (always valid) indices, so that
-            // all 32 are in flight together; out-of-range values become 0
-            const int64_t ic = act ? i : ng - 1;
-            float y[32];
-#pragma unroll
-            for (int u = 0; u < 32; ++u) {
-                const int k = jb + u - 3;
-                const int kc = min(max(k, 0), ns - 1);
-                const float v = (float)__ldg(Y + (int64_t)kc * ng + ic);
-                y[u] = (act && k >= 0 && k < ns) ? v : 0.0f;
-            }
-            float invT = 0.0f, lnT = 0.0f, lnP = 0.0f;
-            if (act && half == 0) {
-                const double t = T[i];
-                invT = (float)(1000.0 / t);
-                lnT = logf((float)t);
-                lnP = logf((float)(P[i] / 1013250.0));
-            }
-            float part = 0.0f;
-#pragma unroll
-            for (int u = 0; u < 32; ++u) {
-                const int k = jb + u - 3;
-                if (k >= 0 && k < ns) part = fmaf(fmaxf(y[u], 0.0f), (float)__ldg(inv_mw + k), part);
-            }
-            sPart[half * kPts + row] = part;
-            __syncthreads();
-            const float lmix = __logf(fmaxf(sPart[row] + sPart[kPts + row], 1e-37f));
-#pragma unroll
-            for (int g = 0; g < 4; ++g) {
-                uint32_t hi[4], lo[4];
-#pragma unroll
-                for (int u = 0; u < 8; u += 2) {
-                    float f[2];
-#pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        const int uu = 8 * g + u + e, j = jb + uu, k = j - 3;
-                        float v = 0.0f;
-                        if (act) {
-                            if (j == 0) {
-                                v = (invT - nrm[0]) * nrm[1];
-                            } else if (j == 1) {
-                                v = (lnT - nrm[2]) * nrm[3];
-                            } else if (j == 2) {
-                                v = (lnP - nrm[4]) * nrm[5];
-                            } else if (k < ns) {
-                                // fast log: ~1e-5 absolute, below the ~2^-16 of the split inputs
-                                const float lx = __logf(fmaxf(y[uu], 1e-30f) * (float)__ldg(inv_mw + k)) - lmix;
-                                v = fminf(fmaxf((lx - nrm[6]) * nrm[7], -6.0f), 6.0f);
-                            }
-                        }
-                        f[e] = v;
-                    }
-                    const bf16 h0 = __float2bfloat16(f[0]), h1 = __float2bfloat16(f[1]);
-                    hi[u / 2] = pack2(h0, h1);
-                    lo[u / 2] = pack2(__float2bfloat16(f[0] - __bfloat162float(h0)),
-                                      __float2bfloat16(f[1] - __bfloat162float(h1)));
-                }
-                const int j0 = jb + 8 * g;
-                *reinterpret_cast<uint4*>(sA + um::kmajor_offset(row, j0, kK1)) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-                *reinterpret_cast<uint4*>(sA + um::kmajor_offset(row, kDin + j0, kK1)) =
-                    make_uint4(lo[0], lo[1], lo[2], lo[3]);
-            }
-        }
-        um::fence_proxy_async();
-        um::fence_before_sync();
-        __syncthreads();
-        um::fence_after_sync();
-        for (int l = 0; l < 4; ++l) {
-            const int K = layer_k(l), N = layer_n(l);
-            if (tid == 0) {
-                const bool ok = um::mbar_wait(&bars[1], wpar);
-                if (ok) {
-                    wpar ^= 1u;
-                    w_pending = false;
-                    um::fence_after_sync();
-                    const uint32_t idesc = um::idesc_bf16(kPts, N);
-                    const uint32_t a = um::smem_addr(sA), b = um::smem_addr(sW);
-                    for (int ks = 0; ks < K / 16; ++ks)
-                        um::mma_bf16(tbase, um::desc_kmajor(a, K, ks), um::desc_kmajor(b, K, ks), idesc,
-                                     ks > 0 ? 1u : 0u);
-                    um::commit(&bars[0]);
-                } else {
-                    *wfail = 1;
-                }
-            }
-            __syncthreads();
-            if (*wfail) {
-                failed = true;
+
+    if (tid >= kCompute) {
+        // ------------------------------------------------------ feature group
+        const int row = tid - kCompute;
+        int j = 0;
+        for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++j) {
+            if (j > 0 && !um::mbar_wait(&bars[3], (uint32_t)((j - 1) & 1))) {
+                *ffail = 1;
                 break;
             }
-            const bool ok = um::mbar_wait(&bars[0], mpar);
-            if (!ok) {
-                *mfail = 1;
-                m_failed = true;
-            } else {
-                mpar ^= 1u;
-            }
-            um::fence_after_sync();
-            if (ok) {
-                // the weights of the next layer (or of the next tile's first
-                // layer) stream in while this epilogue runs
-                if (tid == 0 && (l < 3 || tile + gridDim.x < ntiles)) {
-                    issue_weights(img, l < 3 ? l + 1 : 0, sW, &bars[1]);
-                    w_pending = true;
-                }
-                if (l < 3) {
-                    const float* bl = sBias + kHid * l;
-#pragma unroll 1
-                    for (int c = 128 * ehalf; c < 128 * ehalf + 128; c += 64) {
-                        // one 64-column load, then 64 independent GELUs
-                        uint32_t r[64];
-                        um::tmem_ld64(um::tmem_lane_addr(tbase, g4, c), r);
-#pragma unroll
-                        for (int q = 0; q < 4; ++q)
-                            gelu_store16(r + 16 * q, bl + c + 16 * q, sA + um::kmajor_offset(erow, c + 16 * q, kHid),
-                                         sA + um::kmajor_offset(erow, c + 16 * q + 8, kHid));
-                    }
-                } else {
-                    const float* b4 = sBias + 3 * kHid;
-                    const int64_t i = tile * kPts + erow;
-                    const bool act = i < ng;
-                    const int cL = (ns / 16) * 16;
-                    float v[16];
-                    um::tmem_ld16(um::tmem_lane_addr(tbase, g4, cL), v);
-                    float L = 0.0f;
-#pragma unroll
-                    for (int j = 0; j < 16; ++j)
-                        if (cL + j == ns) L = v[j];
-                    const double scale = exp(lc + ls * (double)(L + b4[ns]));
-#pragma unroll 1
-                    for (int c = 32 * ehalf; c < 32 * ehalf + 32; c += 16) {
-                        um::tmem_ld16(um::tmem_lane_addr(tbase, g4, c), v);
-                        if (act) {
-#pragma unroll
-                            for (int j = 0; j < 16; ++j) {
-                                const int k = c + j;
-                                if (k < ns) W[(int64_t)k * ng + i] = (double)(v[j] + b4[k]) * scale;
-                                else if (k == ns + 1 && est) est[i] = v[j] + b4[k];
-                            }
-                        }
-                    }
+            if (*wfail || *mfail) break;
+            // the inputs of the tile after this one start moving into L2
+            if (warp == kThreads / 32 - 1 && tile + gridDim.x < ntiles) {
+                const int64_t n0 = (tile + gridDim.x) * kPts;
+                const uint32_t bytes = (uint32_t)(min((int64_t)kPts, ng - n0) * 8) & ~15u;
+                for (int r = lane; r < ns + 2 && bytes; r += 32) {
+                    const double* src = r < ns ? Y + (int64_t)r * ng + n0 : (r == ns ? T + n0 : P + n0);
+                    if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) um::bulk_prefetch_l2(src, bytes);
                 }
             }
+            write_features(sF, row, tile, ng, ns, P, T, Y, inv_mw, nrm);
             um::fence_proxy_async();
-            um::fence_before_sync();
-            __syncthreads();
-            um::fence_after_sync();
-            if (*mfail) {
-                failed = true;
-                break;
-            }
+            um::mbar_arrive(&bars[2]);
         }
-    }
-    if (failed) {
-        // drain what this CTA issued (bounded) before tensor memory is freed
+    } else {
+        // ------------------------------------------------------ compute group
+        const int g4 = warp & 3, ehalf = warp >> 2;   // TMEM lane group, column half
+        const int erow = 32 * g4 + lane;
+        const double lc = (double)__ldg(lnorm), ls = (double)__ldg(lnorm + 1);
         if (tid == 0) {
-            atomicExch(&g_sur_err, 1);
-            if (w_pending) um::mbar_wait(&bars[1], wpar);
+            issue_weights(img, 0, sW, &bars[1]);
+            w_pending = true;
         }
-        if (m_failed) um::mbar_wait(&bars[0], mpar);
+        int j = 0;
+        for (int64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x, ++j) {
+            for (int l = 0; l < 4; ++l) {
+                const int K = layer_k(l), N = layer_n(l);
+                if (tid == 0) {
+                    const bool okw = um::mbar_wait(&bars[1], wpar);
+                    if (okw) {
+                        wpar ^= 1u;
+                        w_pending = false;
+                    }
+                    const bool okf = okw && (l != 0 || um::mbar_wait(&bars[2], (uint32_t)(j & 1)));
+                    if (okf) {
+                        um::fence_after_sync();
+                        const uint32_t idesc = um::idesc_bf16(kPts, N);
+                        const uint32_t a = um::smem_addr(l == 0 ? sF : sA), b = um::smem_addr(sW);
+                        for (int ks = 0; ks < K / 16; ++ks)
+                            um::mma_bf16(tbase, um::desc_kmajor(a, K, ks), um::desc_kmajor(b, K, ks), idesc,
+                                         ks > 0 ? 1u : 0u);
+                        um::commit(&bars[0]);
+                    } else {
+                        *wfail = 1;
+                    }
+                }
+                um::bar_sync(1, kCompute);
+                if (*wfail) {
+                    failed = true;
+                    break;
+                }
+                const bool ok = um::mbar_wait(&bars[0], mpar);
+                if (!ok) {
+                    *mfail = 1;
+                    m_failed = true;
+                } else {
+                    mpar ^= 1u;
+                }
+                um::fence_after_sync();
+                if (ok) {
+                    // the first layer has read the features: the feature group
+                    // may write the next tile's
+                    if (l == 0 && tid == 0) um::mbar_arrive(&bars[3]);
+                    // the weights of the next layer (or of the next tile's first
+                    // layer) stream in while this epilogue runs
+                    if (tid == 0 && (l < 3 || tile + gridDim.x < ntiles)) {
+                        issue_weights(img, l < 3 ? l + 1 : 0, sW, &bars[1]);
+                        w_pending = true;
+                    }
+                    if (l < 3) {
+                        const float* bl = bias + kHid * l;
+#pragma unroll 1
+                        for (int c = 128 * ehalf; c < 128 * ehalf + 128; c += 64) {
+                            uint32_t r[64];
+                            um::tmem_ld64(um::tmem_lane_addr(tbase, g4, c), r);
+#pragma unroll
+                            for (int q = 0; q < 4; ++q)
+                                gelu_store16(r + 16 * q, bl + c + 16 * q, sA + um::kmajor_offset(erow, c + 16 * q, kHid),
+                                             sA + um::kmajor_offset(erow, c + 16 * q + 8, kHid));
+                        }
+                    } else {
+                        const float* b4 = bias + 3 * kHid;
+                        const int64_t i = tile * kPts + erow;
+                        const bool act = i < ng;
+                        const int cL = (ns / 16) * 16;
+                        float v[16];
+                        um::tmem_ld16(um::tmem_lane_addr(tbase, g4, cL), v);
+                        float L = 0.0f;
+#pragma unroll
+                        for (int q = 0; q < 16; ++q)
+                            if (cL + q == ns) L = v[q];
+                        const double scale = exp(lc + ls * (double)(L + __ldg(b4 + ns)));
+#pragma unroll 1
+                        for (int c = 32 * ehalf; c < 32 * ehalf + 32; c += 16) {
+                            um::tmem_ld16(um::tmem_lane_addr(tbase, g4, c), v);
+                            if (act) {
+#pragma unroll
+                                for (int q = 0; q < 16; ++q) {
+                                    const int k = c + q;
+                                    if (k < ns) W[(int64_t)k * ng + i] = (double)(v[q] + __ldg(b4 + k)) * scale;
+                                    else if (k == ns + 1 && est) est[i] = v[q] + __ldg(b4 + k);
+                                }
+                            }
+                        }
+                    }
+                }
+                um::fence_proxy_async();
+                um::fence_before_sync();
+                um::bar_sync(1, kCompute);
+                um::fence_after_sync();
+                if (*mfail) {
+                    failed = true;
+                    break;
+                }
+            }
+            if (*ffail) failed = true;
+        }
+        if (failed) {
+            // drain what this group issued (bounded) before tensor memory is freed
+            if (tid == 0) {
+                atomicExch(&g_sur_err, 1);
+                if (w_pending) um::mbar_wait(&bars[1], wpar);
+            }
+            if (m_failed) um::mbar_wait(&bars[0], mpar);
+        }
     }
+    if (tid >= kCompute && *ffail && tid == kCompute) atomicExch(&g_sur_err, 1);
     um::fence_before_sync();
     __syncthreads();
     if (warp == 0) um::tmem_dealloc(tbase, 256);

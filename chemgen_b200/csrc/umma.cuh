@@ -86,6 +86,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint3
     return false;
 }
 
+// Plain arrival on `mbar` (one of the counted arrivals of its phase).
+__device__ __forceinline__ void mbar_arrive(uint64_t* mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(mbar)) : "memory");
+}
+
+// Named barrier `id` (1..15) over the first `nthreads` threads that reach it
+// (a multiple of 32): synchronises a subset of the block's warps.
+__device__ __forceinline__ void bar_sync(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
 // Arrive on `mbar` and add `bytes` to the transaction count its current
 // phase waits for (the bulk copies below complete those bytes).
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
