@@ -49,19 +49,6 @@ __device__ __forceinline__ void split2(double a, int& n, float& f) {
     f = (float)(a - (t - magic));
 }
 
-// FP32 value v (>= 0 or < 0) times 2^k as FP64, by integer exponent arithmetic.
-__device__ __forceinline__ double f32_scaled_to_f64(float v, int k) {
-    const unsigned int b = __float_as_uint(v);
-    const unsigned int ef = (b >> 23) & 0xffu;
-    if (ef == 0u) return 0.0;                         // zero (FP32 subnormals flushed)
-    int e = (int)ef - 127 + k + 1023;
-    e = max(0, min(e, 2047));
-    const unsigned int hi = (b & 0x80000000u) | ((unsigned int)e << 20) | ((b & 0x7fffffu) >> 3);
-    const unsigned int lo = (b & 0x7u) << 29;
-    const double r = __hiloint2double((int)hi, (int)lo);
-    return e == 0 ? 0.0 : (e == 2047 ? __longlong_as_double(0x7ff0000000000000LL | ((long long)(b & 0x80000000u) << 32)) : r);
-}
-
 // 2^k as FP64 for an integer k, built in the exponent field; k is clamped
 // to [-1023, 1023] (2^-1023 encodes as +0).
 __device__ __forceinline__ double exp2i(int k) {
@@ -93,9 +80,8 @@ __device__ __forceinline__ void falloff_blend(float mpr, int npr, float l2m, flo
 
 // q = 2^a * prod  (prod an FP32 product of scaled concentrations, eoff the
 // integer exponent that undoes their scaling): the FP32 value 2^f * prod,
-// converted exactly to FP64, times 2^(n + eoff).  For results in the FP64
-// normal range this is bit-identical to rebuilding the double from the
-// float's fields (f32_scaled_to_f64), in fewer instructions.
+// converted exactly to FP64, times 2^(n + eoff) -- exact for results in the
+// FP64 normal range.
 __device__ __forceinline__ double rate2(double a, float prod, int eoff) {
     int n;
     float f;
