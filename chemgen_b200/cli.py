@@ -32,6 +32,9 @@ def parse_arguments(argv=None):
     ap.add_argument("--yaml_file", help="Cantera YAML mechanism (used instead of --mech)")
     ap.add_argument("--output", required=True, help="output file")
     ap.add_argument("--language", choices=["cuda"], default="cuda")
+    ap.add_argument("--precision", choices=["fp64", "mixed", "both"], default="both",
+                    help="kernels to generate: FP64 (the reference's arithmetic), mixed (FP32 rate math, "
+                         "<= 1e-6 normwise) or both; a mode not generated runs on the table-driven kernels")
     ap.add_argument("--name", help="identifier for the generated module (default: mechanism file stem)")
     ap.add_argument("--reference-compat", action="store_true",
                     help="drop Lindemann/SRI/chemically-activated reactions as the reference's parser does")
@@ -62,14 +65,14 @@ def main(argv=None) -> int:
         return 0
     from . import emit_cuda
     with open(args.output, "w") as f:
-        f.write(emit_cuda.emit(mech, name=args.name))
+        f.write(emit_cuda.emit(mech, name=args.name, precision=args.precision))
     with open(stem + ".blob", "wb") as f:
         f.write(blob)
     print(f"getrates kernels ({mech.ns} species, {mech.nr} reactions, {mech.counts()}) written to {args.output}")
     if mech.dropped:
         print(f"dropped {len(mech.dropped)} reactions: {mech.dropped[:5]}")
     if args.build:
-        so = emit_cuda.build_module(mech, out=stem + ".so", name=args.name)
+        so = emit_cuda.build_module(mech, out=stem + ".so", name=args.name, precision=args.precision)
         print(f"compiled module {so}")
     return 0
 

@@ -474,44 +474,62 @@ def choose_block(ns: int) -> int:
     return 256 if 256 * per <= SMEM_BUDGET else 128
 
 
+PRECISIONS = {"fp64": (True, False), "mixed": (False, True), "both": (True, True)}
+
+
 def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = None,
-         sync_every: int = SYNC_EVERY) -> str:
+         sync_every: int = SYNC_EVERY, precision: str = "both") -> str:
+    """CUDA source of the mechanism's kernels: `precision` selects the FP64
+    kernel, the mixed one or both; a mode without a generated kernel runs on
+    the table-driven kernels."""
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+    want64, want32 = PRECISIONS[precision]
     blob = pack(mech).to_blob()
     fp = fingerprint(blob)
     block = block or choose_block(mech.ns)
     em = _Emitter(mech, block, sync_every)
     ident = "".join(ch if ch.isalnum() else "_" for ch in (name or mech.name))
     src = [
-        f"// Generated by chemgen_b200 (generate_chemistry.py --language cuda) for mechanism '{mech.name}':",
+        f"// Generated by chemgen_b200 (generate_chemistry.py --language cuda --precision {precision}) for mechanism '{mech.name}':",
         f"// {mech.ns} species, {mech.nr} reactions {mech.counts()}.",
         f"// Blob fingerprint 0x{fp:016x}.  Target: sm_100a.",
         '#include "gen_common.cuh"',
         '#include "cg_math.cuh"',
         "using cgg::rcp;",
         "namespace {",
-        em.kernel(False),
-        "",
-        em.kernel(True),
-        "",
+    ]
+    attrs, dispatch = [], []
+    if want64:
+        src += [em.kernel(False), ""]
+        attrs.append(f"cudaFuncSetAttribute(cg_gen_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, "
+                     f"{em.smem_bytes(False)}) != cudaSuccess")
+        dispatch.append(f"  if (mode == CHEMGEN_MODE_FP64) {{ cg_gen_fp64<<<blocks, {block}, {em.smem_bytes(False)}, st>>>"
+                        "(P, T, Y, wdot, ng); return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA; }")
+    if want32:
+        src += [em.kernel(True), ""]
+        attrs.append(f"cudaFuncSetAttribute(cg_gen_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, "
+                     f"{em.smem_bytes(True)}) != cudaSuccess")
+        dispatch.append(f"  if (mode == CHEMGEN_MODE_MIXED) {{ cg_gen_mixed<<<blocks, {block}, {em.smem_bytes(True)}, st>>>"
+                        "(P, T, Y, wdot, ng); return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA; }")
+    modes = (1 if want64 else 0) | (2 if want32 else 0)
+    src += [
         "int launch(int mode, const double* P, const double* T, int64_t ng, const double* Y, double* wdot, void* s) {",
         "  if (ng <= 0) return CHEMGEN_OK;",
         "  static bool attrs = false;",
         "  if (!attrs) {",
-        f"    if (cudaFuncSetAttribute(cg_gen_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, {em.smem_bytes(False)}) != cudaSuccess ||",
-        f"        cudaFuncSetAttribute(cg_gen_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, {em.smem_bytes(True)}) != cudaSuccess)",
+        "    if (" + " ||\n        ".join(attrs) + ")",
         "      return CHEMGEN_ERR_CUDA;",
         "    attrs = true;",
         "  }",
         f"  const unsigned blocks = (unsigned)((ng + {block - 1}) / {block});",
         "  cudaStream_t st = (cudaStream_t)s;",
-        f"  if (mode == CHEMGEN_MODE_FP64) cg_gen_fp64<<<blocks, {block}, {em.smem_bytes(False)}, st>>>(P, T, Y, wdot, ng);",
-        f"  else if (mode == CHEMGEN_MODE_MIXED) cg_gen_mixed<<<blocks, {block}, {em.smem_bytes(True)}, st>>>(P, T, Y, wdot, ng);",
-        "  else return CHEMGEN_ERR_INVALID_ARGUMENT;",
-        "  return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA;",
+    ] + dispatch + [
+        "  return CHEMGEN_ERR_INVALID_ARGUMENT;",
         "}",
         "",
         "struct Register {",
-        f"  Register() {{ chemgen_register_kernels(0x{fp:016x}ull, {mech.ns}, {mech.nr}, 3u, &launch); }}",
+        f"  Register() {{ chemgen_register_kernels(0x{fp:016x}ull, {mech.ns}, {mech.nr}, {modes}u, &launch); }}",
         "} register_once;",
         "}  // namespace",
         "",

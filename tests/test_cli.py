@@ -43,3 +43,18 @@ def test_getrates_cuda_emits_compilable_source(tmp_path, src):
     r = subprocess.run([nvcc()] + ARCH + FLAGS + ["-I", os.path.join(REPO, "chemgen_b200", "csrc"), "-c",
                         str(out), "-o", str(obj)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-2000:]
+
+
+@pytest.mark.parametrize("precision,has64,has32,mask", [("fp64", True, False, 1), ("mixed", False, True, 2),
+                                                         ("both", True, True, 3)])
+def test_precision_selects_the_generated_kernels(tmp_path, precision, has64, has32, mask):
+    from chemgen_b200 import cli
+    out = tmp_path / "k.cu"
+    src_yaml = tmp_path / "m.json"
+    from chemgen_b200 import synthetic
+    src_yaml.write_text(synthetic.h2o2_10sp().to_json())
+    assert cli.main(["--mode", "getrates", "--mech", str(src_yaml), "--output", str(out), "--language", "cuda",
+                     "--precision", precision]) == 0
+    text = out.read_text()
+    assert ("cg_gen_fp64<<<" in text) == has64 and ("cg_gen_mixed<<<" in text) == has32
+    assert f", {mask}u, &launch)" in text
