@@ -471,8 +471,10 @@ cudaError_t mixed_prepare(const DevMech& m, const cg_mech_view& v, int device, M
     p->g_smem = with_g <= limit ? 1 : 0;
     // FP32 accumulation runs over `group` chunks (16 reactions each) before
     // the partial sums are added into the FP64 output: 64 reactions for small
-    // mechanisms, 512 for large ones (where each flush moves ns doubles)
-    p->group = npad <= 128 ? 4 : 32;
+    // mechanisms (GRI30 needs it for 1e-6), the whole mechanism for large
+    // ones, whose output does not fit in L2 and would otherwise be read back
+    // from DRAM at every flush (348/2163: 3.5e-7 with one flush)
+    p->group = npad <= 128 ? 4 : nchunk;
     p->smem = p->g_smem ? with_g : base;
     // resident CTAs per SM, limited by shared memory and by 512 TMEM columns
     int per_sm = (int)(prop.sharedMemPerMultiprocessor / (p->smem + 1024));
