@@ -205,7 +205,7 @@ def rank_states(ns: int, ng: int, rank: int):
 
 def surrogate_leg(args, gm, stream):
     """Train the MLP surrogate on exact-kernel samples, then report its
-    accuracy (normwise, judged by the FP64 kernel), the fused kernel's
+    accuracy (normwise, measured against the FP64 kernel), the fused kernel's
     points/s, the error gate's fallback rate and what the surrogate with
     fallback gains over the exact kernels at that tolerance."""
     import torch

@@ -9,7 +9,7 @@ length (ln |w|_2 - c) / s (column ns) and an estimate of log10 of the
 network's own normwise error at that point (column ns + 1).  Because the
 normwise error of a decoded prediction is, to first order,
 max_k |du_k| / max_k |u_k| + |d ln |w|_2|, the regression loss weighs the
-outputs the way the error gate judges them.  BF16 weights (FP32 master
+outputs the way the error gate measures them.  BF16 weights (FP32 master
 copies) and FP32 accumulation.
 
 Training runs entirely on this package's CUDA kernels (chemgen_mlp_* in
@@ -21,7 +21,7 @@ step is captured as a CUDA graph and replayed.  The training data are
 Inference (`SurrogateGetrates`): the network predicts wdot and its error
 estimate; a point falls back to the exact kernel when its inputs leave the
 training ranges or the estimate exceeds the tolerance.  The exact kernel is
-also the judge used to report the surrogate's accuracy.
+also the reference used to report the surrogate's accuracy.
 
 The reference has no surrogate; its chemgen/chemistry_nn.py:15-85 torch
 prototype (log-space Arrhenius layers) never ran.

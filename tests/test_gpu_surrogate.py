@@ -1,6 +1,6 @@
 """The learned surrogate: kernel products and gradients against the CPU
 oracle, training on samples from the exact kernel, and what the trained
-network gains over the exact kernel alone at its achieved tolerance (judged
+network gains over the exact kernel alone at its achieved tolerance (measured
 by the FP64 kernel)."""
 import math
 
@@ -138,7 +138,7 @@ def test_surrogate_trains_and_gains_over_exact_kernel():
     info = sur.fit(S.TrainConfig(samples=4_000_000, batch=2048, epochs=12, error_head_epochs=1))
     print(info, sur.history)
     assert sur.history[-1] < 0.05 * sur.history[0]
-    # held-out states, judged by the FP64 kernel
+    # held-out states, measured against the FP64 kernel
     ng = 1 << 18
     gen = torch.Generator(device="cuda").manual_seed(99)
     P, T, Y = sur.sample_states(ng, gen)
