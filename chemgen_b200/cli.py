@@ -68,6 +68,14 @@ def main(argv=None) -> int:
         f.write(emit_cuda.emit(mech, name=args.name, precision=args.precision))
     with open(stem + ".blob", "wb") as f:
         f.write(blob)
+    # the op inventory of one point's rate law, the work per point of the
+    # roofline (transcendentals counted separately, weighted by their measured
+    # FMA-slot cost when the roofline is computed)
+    import json
+    from . import ops
+    with open(stem + ".ops.json", "w") as f:
+        json.dump({"mechanism": mech.name, "ns": mech.ns, "nr": mech.nr, "ops_per_point": ops.inventory(mech),
+                   "hbm_bytes_per_point": ops.bytes_per_point(mech.ns)}, f, indent=1)
     print(f"getrates kernels ({mech.ns} species, {mech.nr} reactions, {mech.counts()}) written to {args.output}")
     if mech.dropped:
         print(f"dropped {len(mech.dropped)} reactions: {mech.dropped[:5]}")

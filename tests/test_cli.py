@@ -58,3 +58,8 @@ def test_precision_selects_the_generated_kernels(tmp_path, precision, has64, has
     text = out.read_text()
     assert ("cg_gen_fp64<<<" in text) == has64 and ("cg_gen_mixed<<<" in text) == has32
     assert f", {mask}u, &launch)" in text
+    import json
+    from chemgen_b200 import ops
+    rec = json.loads((tmp_path / "k.ops.json").read_text())
+    assert rec["ns"] == 10 and rec["nr"] == 27 and rec["hbm_bytes_per_point"] == 176
+    assert rec["ops_per_point"] == ops.inventory(synthetic.h2o2_10sp())
