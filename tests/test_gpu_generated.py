@@ -90,3 +90,27 @@ def test_generated_mixed_edge_states():
         assert np.all(np.isfinite(w))
         e = oracle.errors(w, r["wdot"], r["S"])
         assert e["norm_max"] <= tol, (mode, e)
+
+
+def test_fp64_only_module_leaves_mixed_on_the_table_kernels(tmp_path):
+    """A module generated with precision="fp64" registers the FP64 mode only:
+    mixed runs on the table-driven (tensor-core) kernel, both stay in parity.
+    (A mechanism no other test loads: kernel registration is process-wide.)"""
+    import ctypes
+    import torch
+    from chemgen_b200 import emit_cuda
+    from chemgen_b200.runtime import lib
+    mech = synthetic.synthetic_mechanism(12, 30, 3, 2, seed=77, name="synthetic_12_30_s77")
+    so = emit_cuda.build_module(mech, out=str(tmp_path / "fp64only.so"), precision="fp64")
+    lib()
+    ctypes.CDLL(so, mode=ctypes.RTLD_GLOBAL)
+    blob = pack.pack(mech).to_blob()
+    gm = GpuMechanism(blob)
+    assert gm.kernel_kind("fp64") == "generated" and gm.kernel_kind("mixed") == "table"
+    P, T, Y = synthetic.states(mech.ns, 3000, seed=5)
+    S = oracle.rates(blob, P, T, Y, mech.nr)["S"]
+    w_ref = oracle.getrates(blob, P, T, Y)
+    Pd, Td, Yd = (torch.from_numpy(x).cuda() for x in (P, T, Y))
+    e64 = oracle.errors(gm.getrates(Pd, Td, Yd, mode="fp64").cpu().numpy(), w_ref, S)
+    emx = oracle.errors(gm.getrates(Pd, Td, Yd, mode="mixed").cpu().numpy(), w_ref, S)
+    assert e64["norm_max"] <= 1e-10 and emx["norm_max"] <= 1e-6, (e64, emx)
