@@ -44,6 +44,21 @@ constexpr int kTile = 128;       // points per CTA tile (TMEM lanes)
 constexpr int kChunk = 16;       // reactions per MMA chunk (MMA K)
 constexpr int kABytes = kTile * kChunk * 2;   // one BF16 A split tile
 
+// Pre-decoded record of a standard or three-body reaction with at most three
+// molecules per side (the common case), built once per plan on the device:
+// log2-space Arrhenius constants and the species of each molecule, padded with
+// the dummy species ns (C = 1, G = 0), so that the rate needs no decoding.
+struct __align__(16) TcFast {
+    double l2A, b, th2;          // log2|A|, b, (Ea/Rc) log2 e
+    unsigned short sr[3], sp[3]; // reactant / product molecules (species ns = none)
+    unsigned char ordf, ordb;    // concentration factors of each side (M included)
+    unsigned char flags;         // kFastOn | kFastRev | kFastThird | kFastNeg
+    unsigned char pad0;
+    int pad1[2];
+};
+static_assert(sizeof(TcFast) == 48, "TcFast must stay 48 bytes");
+constexpr unsigned kFastOn = 1, kFastRev = 2, kFastThird = 4, kFastNeg = 8;
+
 struct MixedPlan {
     int ns = 0, nr = 0, npad = 0, nhalf = 0, nchunk = 0;
     uint32_t tcols = 0;
@@ -54,6 +69,7 @@ struct MixedPlan {
     int nt = 1;             // threads per point (blockDim = 128 nt)
     void* dbuf = nullptr;
     const __nv_bfloat16* nu = nullptr;
+    const TcFast* fast = nullptr;
     int* err = nullptr;
 };
 
@@ -262,6 +278,74 @@ __device__ float rate_of_progress(const DevMech& m, int r, const TileCtx& c, int
     return sgn * q;
 }
 
+// Net rate of progress of a pre-decoded reaction (TcFast) at point `tid`, FP32.
+__device__ __forceinline__ float rate_fast(const DevMech& m, int r, const TcFast& F, const TileCtx& c, int tid) {
+    const double a = fma(F.b, c.lnT2, F.l2A) - F.th2 * c.invT;
+    float Ms = 1.0f;
+    if (F.flags & kFastThird) {
+        Ms = c.ctot32;
+        for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
+            Ms = fmaf((float)__ldg(m.eff_val + e), c.C[__ldg(m.eff_sp + e) * kTile + tid], Ms);
+    }
+    const float cf = c.C[F.sr[0] * kTile + tid] * c.C[F.sr[1] * kTile + tid] * c.C[F.sr[2] * kTile + tid] * Ms;
+    float q = rate32(a, cf, -32 * (int)F.ordf);
+    if (F.flags & kFastRev) {
+        const double g = (c.G[F.sr[0] * kTile + tid] + c.G[F.sr[1] * kTile + tid] + c.G[F.sr[2] * kTile + tid]) -
+                         (c.G[F.sp[0] * kTile + tid] + c.G[F.sp[1] * kTile + tid] + c.G[F.sp[2] * kTile + tid]);
+        const float cb = c.C[F.sp[0] * kTile + tid] * c.C[F.sp[1] * kTile + tid] * c.C[F.sp[2] * kTile + tid] * Ms;
+        q -= rate32(a + g, cb, -32 * (int)F.ordb);
+    }
+    return (F.flags & kFastNeg) ? -q : q;
+}
+
+__device__ __forceinline__ TcFast load_fast(const TcFast* p) {
+    const int4* q = reinterpret_cast<const int4*>(p);
+    TcFast f;
+    int4* d = reinterpret_cast<int4*>(&f);
+    d[0] = __ldg(q);
+    d[1] = __ldg(q + 1);
+    d[2] = __ldg(q + 2);
+    return f;
+}
+
+// One TcFast per reaction (flags 0 where the generic path is needed).
+__global__ void build_fast_kernel(DevMech m, TcFast* out) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= m.nr) return;
+    const DRxn R = load_rxn(m.rxn + r);
+    int kind = CG_STANDARD;
+    while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
+    TcFast f;
+    f.l2A = R.lnA * kLog2eD;
+    f.b = R.b;
+    f.th2 = R.theta * kLog2eD;
+    f.pad0 = 0;
+    f.pad1[0] = f.pad1[1] = 0;
+    f.flags = 0;
+    f.ordf = f.ordb = 0;
+    for (int j = 0; j < 3; ++j) f.sr[j] = f.sp[j] = (unsigned short)m.ns;
+    bool ok = (kind == CG_STANDARD || kind == CG_THIRD_BODY) && (R.flags & kFCompact) && R.sgn != 0.0;
+    int nf = 0, nb = 0;
+    for (int j = 0; ok && j < R.nre; ++j)
+        for (int k = 0; k < slot_nu(R.sp[j]); ++k) {
+            if (nf == 3) ok = false;
+            else f.sr[nf++] = (unsigned short)slot_species(R.sp[j]);
+        }
+    for (int j = 0; ok && j < R.npr; ++j)
+        for (int k = 0; k < slot_nu(R.sp[3 + j]); ++k) {
+            if (nb == 3) ok = false;
+            else f.sp[nb++] = (unsigned short)slot_species(R.sp[3 + j]);
+        }
+    if (ok) {
+        const bool third = kind == CG_THIRD_BODY;
+        f.ordf = (unsigned char)(nf + (third ? 1 : 0));
+        f.ordb = (unsigned char)(nb + (third ? 1 : 0));
+        f.flags = (unsigned char)(kFastOn | ((R.flags & CG_F_REVERSIBLE) ? kFastRev : 0) | (third ? kFastThird : 0) |
+                                  (R.sgn < 0.0 ? kFastNeg : 0));
+    }
+    out[r] = f;
+}
+
 // NT threads share each of the tile's 128 points (blockDim = 128 NT): they
 // split the species of the prologue (their partial sums meet in shared
 // memory), the 16 reactions of each chunk, and the accumulator columns of
@@ -269,7 +353,8 @@ __device__ float rate_of_progress(const DevMech& m, int r, const TileCtx& c, int
 // no per-species registers.
 template <bool GS, int NT>
 __global__ void __launch_bounds__(kTile * NT, 1)
-    getrates_tc_kernel(DevMech m, const __nv_bfloat16* __restrict__ nu, int npad, int nhalf, int nchunk, uint32_t tcols,
+    getrates_tc_kernel(DevMech m, const __nv_bfloat16* __restrict__ nu, const TcFast* __restrict__ fast, int npad,
+                       int nhalf, int nchunk, uint32_t tcols,
                        const double* __restrict__ P, const double* __restrict__ Tg, const double* __restrict__ Y,
                        double* __restrict__ wdot, int64_t ng, double* __restrict__ gscratch, int* err, int group) {
     extern __shared__ __align__(1024) unsigned char sm[];
@@ -278,10 +363,11 @@ __global__ void __launch_bounds__(kTile * NT, 1)
     const int ns = m.ns;
     unsigned char* sA = sm;                                    // [2 buffers][3 splits][128 x 16] BF16
     unsigned char* sB = sm + 6 * kABytes;                      // [2 buffers][npad x 16] BF16
-    float* sC = reinterpret_cast<float*>(sB + 2 * npad * 32);  // [ns][128]
-    double* sG = GS ? reinterpret_cast<double*>(sC + ns * kTile) : gscratch + (int64_t)blockIdx.x * ns * kTile;
-    double* sRed = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(sC) + ns * kTile * 4 +
-                                             (GS ? ns * kTile * 8 : 0));   // [NT][128] partial sums
+    const int rows = ns + 1;                                   // species + the dummy row of TcFast
+    float* sC = reinterpret_cast<float*>(sB + 2 * npad * 32);  // [rows][128]
+    double* sG = GS ? reinterpret_cast<double*>(sC + rows * kTile) : gscratch + (int64_t)blockIdx.x * rows * kTile;
+    double* sRed = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(sC) + rows * kTile * 4 +
+                                             (GS ? rows * kTile * 8 : 0));   // [NT][128] partial sums
     uint64_t* mbar = reinterpret_cast<uint64_t*>(sRed + NT * kTile);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
     if (tid == 0) {
@@ -343,6 +429,10 @@ __global__ void __launch_bounds__(kTile * NT, 1)
         const double lpfac2 = -6.35856916300311 - c.lnT2;   // log2(Patm/R0) - log2 T
         for (int k = sub; k < ns; k += NT)
             sG[k * kTile + pt] = fma(species_smh(m.thermo, k, c.T, c.lnT, c.invT), kLog2eD, lpfac2);
+        if (sub == 0) {
+            sC[ns * kTile + pt] = 1.0f;     // dummy species of TcFast: a factor 1 ...
+            sG[ns * kTile + pt] = 0.0;      // ... and no Gibbs term
+        }
         __syncthreads();
         bool first_group = true;
         for (int ch = 0; ch < nchunk && ok; ++ch) {
@@ -361,7 +451,11 @@ __global__ void __launch_bounds__(kTile * NT, 1)
             unsigned char* a0 = sA + buf * 3 * kABytes;
             for (int j = sub; j < kChunk; j += NT) {
                 const int r = ch * kChunk + j;
-                float q = (r < m.nr) ? rate_of_progress(m, r, c, pt) : 0.0f;
+                float q = 0.0f;
+                if (r < m.nr) {
+                    const TcFast F = load_fast(fast + r);
+                    q = (F.flags & kFastOn) ? rate_fast(m, r, F, c, pt) : rate_of_progress(m, r, c, pt);
+                }
                 if (!act) q = 0.0f;
                 const __nv_bfloat16 h = __float2bfloat16_rn(q);
                 const float r1 = q - __bfloat162float(h);
@@ -435,7 +529,7 @@ const void* kernel_for(int g_smem, int nt) {
 template <bool GS, int NT>
 cudaError_t launch_tc(const MixedPlan* p, const DevMech& m, const double* P, const double* T, const double* Y,
                       double* wdot, int64_t ng, double* scratch, int64_t grid, cudaStream_t s) {
-    getrates_tc_kernel<GS, NT><<<(unsigned)grid, kTile * NT, p->smem, s>>>(m, p->nu, p->npad, p->nhalf, p->nchunk,
+    getrates_tc_kernel<GS, NT><<<(unsigned)grid, kTile * NT, p->smem, s>>>(m, p->nu, p->fast, p->npad, p->nhalf, p->nchunk,
                                                                            p->tcols, P, T, Y, wdot, ng, scratch,
                                                                            p->err, p->group);
     return cudaGetLastError();
@@ -454,8 +548,9 @@ cudaError_t mixed_prepare(const DevMech& m, const cg_mech_view& v, int device, M
     while ((int)tcols < npad) tcols <<= 1;
     const int nchunk = (nr + kChunk - 1) / kChunk;
     // the largest share count is planned for; the [nt][128] partial-sum slots follow the state
-    const size_t base = 6 * (size_t)kABytes + 2 * (size_t)npad * 32 + (size_t)ns * kTile * 4 + 4 * kTile * 8 + 32;
-    const size_t with_g = base + (size_t)ns * kTile * 8;
+    const size_t rows = (size_t)ns + 1;                       // + the dummy row of TcFast
+    const size_t base = 6 * (size_t)kABytes + 2 * (size_t)npad * 32 + rows * kTile * 4 + 4 * kTile * 8 + 32;
+    const size_t with_g = base + rows * kTile * 8;
     cudaDeviceProp prop;
     cudaError_t e = cudaGetDeviceProperties(&prop, device);
     if (e != cudaSuccess) return e;
@@ -522,7 +617,9 @@ cudaError_t mixed_prepare(const DevMech& m, const cg_mech_view& v, int device, M
         delete p;
         return cudaErrorNotSupported;                  // coefficients not exact in BF16
     }
-    const size_t bytes = img.size() * sizeof(__nv_bfloat16) + 256;
+    const size_t img_bytes = (img.size() * sizeof(__nv_bfloat16) + 255) / 256 * 256;
+    const size_t fast_bytes = (size_t)nr * sizeof(TcFast);
+    const size_t bytes = img_bytes + fast_bytes + 256;
     e = cudaMalloc(&p->dbuf, bytes);
     if (e == cudaSuccess) e = cudaMemcpy(p->dbuf, img.data(), img.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset((char*)p->dbuf + bytes - 256, 0, 256);
@@ -534,6 +631,17 @@ cudaError_t mixed_prepare(const DevMech& m, const cg_mech_view& v, int device, M
         return e;
     }
     p->nu = (const __nv_bfloat16*)p->dbuf;
+    p->fast = (const TcFast*)((char*)p->dbuf + img_bytes);
+    if (nr > 0) {
+        build_fast_kernel<<<(nr + 127) / 128, 128>>>(m, (TcFast*)p->fast);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) {
+            cudaFree(p->dbuf);
+            delete p;
+            return e;
+        }
+    }
     p->err = (int*)((char*)p->dbuf + bytes - 256);
     *out = p;
     return cudaSuccess;
@@ -549,7 +657,7 @@ size_t mixed_workspace_bytes(const MixedPlan* p, int64_t ng) {
     if (!p || p->g_smem) return 0;
     int64_t tiles = (ng + kTile - 1) / kTile;
     int64_t grid = std::min<int64_t>(tiles, p->grid);
-    return (size_t)grid * p->ns * kTile * sizeof(double);
+    return (size_t)grid * (p->ns + 1) * kTile * sizeof(double);
 }
 
 cudaError_t launch_getrates_mixed(const MixedPlan* p, const DevMech& m, const double* P, const double* T,
@@ -559,7 +667,7 @@ cudaError_t launch_getrates_mixed(const MixedPlan* p, const DevMech& m, const do
     int64_t tiles = (ng + kTile - 1) / kTile;
     int64_t grid = std::min<int64_t>(tiles, p->grid);
     if (!p->g_smem) {
-        const int64_t fit = (int64_t)(scratch_bytes / ((size_t)p->ns * kTile * sizeof(double)));
+        const int64_t fit = (int64_t)(scratch_bytes / ((size_t)(p->ns + 1) * kTile * sizeof(double)));
         grid = std::min<int64_t>(grid, fit);
         if (grid < 1 || !scratch) return cudaErrorInvalidValue;
     }
