@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--head", default="auto", choices=["auto", "fp64", "mixed", "mixed_tc"],
                     help="headline mode; auto = the fastest mode within 1e-6 (under a profiler, whose "
                          "serialised launches distort the timings that choose it, pass it explicitly)")
+    ap.add_argument("--configs-only", action="store_true",
+                    help="run only the other configurations and print them (for profiling their kernels)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other configurations (real GRI30, mini-app states, 348/2163, Jacobian)")
     return ap.parse_args()
@@ -353,6 +355,10 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
+    if args.configs_only:
+        if rank == 0:
+            print(json.dumps({"configs": other_configs(args, torch.cuda.current_stream())}), flush=True)
+        return
     mech = synthetic.gri_shape()
     blob = pack.pack(mech).to_blob()
     gm = GpuMechanism(mech, device=local_rank, generated=not args.table)
