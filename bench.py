@@ -312,6 +312,21 @@ def other_configs(args, stream):
     legs["mixed"]["tensor"] = {"dense_flop_per_point": dense, "dense_tflops": tf, "bf16_peak_tflops": bf16,
                                "frac_of_bf16_peak": tf / bf16, "sparse_equivalent_flop_per_point": 2.0 * nnz,
                                "note": "BF16 x3 split of q: 3 MMAs of M=128, N=npad, K=16 per 16-reaction chunk"}
+    # per-species error of the tensor-core mixed kernel against the FP64 kernel (itself within 1e-10 of
+    # the oracle): max over points of |dW_k| relative to the species' own largest |W_k|, and relative to
+    # the point's largest |W| (the normwise measure, split by species)
+    W64 = torch.empty_like(Y)
+    Wm = torch.empty_like(Y)
+    gm.getrates(P, T, Y, out=W64, mode="fp64", stream=stream)
+    gm.getrates(P, T, Y, out=Wm, mode="mixed", stream=stream)
+    dW = (Wm - W64).abs()
+    own = (dW.max(dim=1).values / W64.abs().max(dim=1).values.clamp_min(1e-300)).cpu().numpy()
+    nrm = (dW / W64.abs().max(dim=0).values.clamp_min(1e-300)).max(dim=1).values.cpu().numpy()
+    legs["mixed"]["err_per_species"] = {
+        "relative_to_species_max": [float(f"{x:.2g}") for x in own],
+        "relative_to_point_max": [float(f"{x:.2g}") for x in nrm],
+        "worst_species": [mech_sp for mech_sp in (big.species[int(k)].name for k in np.argsort(-nrm)[:5])]}
+    del W64, Wm, dW
     out["c3_348_2163"] = dict(points=n3, ns=big.ns, nr=big.nr, **legs)
     del P, T, Y
     # analytic Jacobian at 65536 points on the headline mechanism
