@@ -89,5 +89,105 @@ __device__ __forceinline__ double rate2(double a, float prod, int eoff) {
     return (double)(ex2f(f) * prod) * exp2i(n + eoff);
 }
 
+// ------------------------------------------------------- tensor memory
+// When shared memory cannot hold both per-point arrays for the block size
+// the kernel wants, the FP64 kernel keeps EGp in tensor memory instead: each
+// thread owns one lane (warp w reaches lanes 32 (w % 4) .. 32 (w % 4) + 31)
+// and, for warp slot w / 4, 2 ns consecutive 32-bit columns, species k at
+// columns 2k, 2k+1 (low, high word).  The tcgen05 ld/st are warp-collective;
+// the generated kernels call them from straight-line code that every thread
+// of the warp executes, and each helper first reconverges the warp
+// (__syncwarp) in case a rare special-argument path of cg_log diverged it.
+
+// Allocates `ncols` columns for the block (warp 0), publishes the base
+// through shared memory and orders it for all threads.
+__device__ __forceinline__ uint32_t tm_alloc(uint32_t* slot, uint32_t ncols) {
+    if ((threadIdx.x >> 5) == 0) {
+        const uint32_t s = (uint32_t)__cvta_generic_to_shared(slot);
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s), "r"(ncols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    return *slot;
+}
+
+__device__ __forceinline__ void tm_free(uint32_t base, uint32_t ncols) {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(ncols) : "memory");
+    }
+}
+
+// This thread's first column: lane quadrant of the warp, column slot w / 4.
+__device__ __forceinline__ uint32_t tm_thread_base(uint32_t base, int cols_per_slot) {
+    const int w = threadIdx.x >> 5;
+    return base + ((uint32_t)(32 * (w & 3)) << 16) + (uint32_t)((w >> 2) * cols_per_slot);
+}
+
+__device__ __forceinline__ void tm_st(uint32_t a, double v) {
+    __syncwarp();
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(a), "r"(__double2loint(v)),
+                 "r"(__double2hiint(v)));
+}
+
+__device__ __forceinline__ void tm_wait_st() {
+    __syncwarp();
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// Loads of 1..4 doubles, each batch completed by one wait inside the same
+// asm so that no register is read before its load has landed.
+__device__ __forceinline__ void tm_ld(uint32_t a0, double& v0) {
+    uint32_t l0, h0;
+    __syncwarp();
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];\n\t"
+                 "tcgen05.wait::ld.sync.aligned;"
+                 : "=r"(l0), "=r"(h0) : "r"(a0));
+    v0 = __hiloint2double((int)h0, (int)l0);
+}
+__device__ __forceinline__ void tm_ld(uint32_t a0, uint32_t a1, double& v0, double& v1) {
+    uint32_t l0, h0, l1, h1;
+    __syncwarp();
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%4];\n\t"
+                 "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%2, %3}, [%5];\n\t"
+                 "tcgen05.wait::ld.sync.aligned;"
+                 : "=r"(l0), "=r"(h0), "=r"(l1), "=r"(h1) : "r"(a0), "r"(a1));
+    v0 = __hiloint2double((int)h0, (int)l0);
+    v1 = __hiloint2double((int)h1, (int)l1);
+}
+__device__ __forceinline__ void tm_ld(uint32_t a0, uint32_t a1, uint32_t a2, double& v0, double& v1, double& v2) {
+    uint32_t l0, h0, l1, h1, l2, h2;
+    __syncwarp();
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%6];\n\t"
+                 "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%2, %3}, [%7];\n\t"
+                 "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%4, %5}, [%8];\n\t"
+                 "tcgen05.wait::ld.sync.aligned;"
+                 : "=r"(l0), "=r"(h0), "=r"(l1), "=r"(h1), "=r"(l2), "=r"(h2) : "r"(a0), "r"(a1), "r"(a2));
+    v0 = __hiloint2double((int)h0, (int)l0);
+    v1 = __hiloint2double((int)h1, (int)l1);
+    v2 = __hiloint2double((int)h2, (int)l2);
+}
+__device__ __forceinline__ void tm_ld(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, double& v0, double& v1,
+                                      double& v2, double& v3) {
+    uint32_t l0, h0, l1, h1, l2, h2, l3, h3;
+    __syncwarp();
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%8];\n\t"
+                 "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%2, %3}, [%9];\n\t"
+                 "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%4, %5}, [%10];\n\t"
+                 "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%6, %7}, [%11];\n\t"
+                 "tcgen05.wait::ld.sync.aligned;"
+                 : "=r"(l0), "=r"(h0), "=r"(l1), "=r"(h1), "=r"(l2), "=r"(h2), "=r"(l3), "=r"(h3)
+                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3));
+    v0 = __hiloint2double((int)h0, (int)l0);
+    v1 = __hiloint2double((int)h1, (int)l1);
+    v2 = __hiloint2double((int)h2, (int)l2);
+    v3 = __hiloint2double((int)h3, (int)l3);
+}
+
 }  // namespace cgg
 

@@ -34,6 +34,8 @@ CSCALE_LOG2 = 32          # mixed: concentrations are stored as C * 2^32 in FP32
 MAX_REG_SPECIES = 72
 SYNC_EVERY = 48           # reactions between block barriers (B200 sweep at 53/325: 2..64, best 48-64)
 SMEM_BUDGET = 220 * 1024  # dynamic shared memory per block
+REG_FILE = 65536          # 32-bit registers per SM
+MAX_BLOCK = 512           # 16 warps; beyond this the 53-species kernels spill heavily
 
 
 def fingerprint(blob: bytes) -> int:
@@ -59,7 +61,7 @@ def _f(x: float) -> str:
 
 
 class _Emitter:
-    def __init__(self, mech: Mechanism, block: int, sync_every: int = SYNC_EVERY):
+    def __init__(self, mech: Mechanism, block: int, sync_every: int = SYNC_EVERY, tmem: bool = False):
         self.sync_every = sync_every
         self.mech = mech
         self.ns = mech.ns
@@ -67,13 +69,39 @@ class _Emitter:
         self.block = block
         self.reg_w = self.ns <= MAX_REG_SPECIES
         self.has_m = any(r.uses_m for r in mech.reactions)
+        # FP64 kernel only: EGp in tensor memory instead of shared memory
+        self.tmem = tmem
+        self._eloc: Dict[str, str] = {}
 
     # ------------------------------------------------------------- helpers
     def C(self, sp: str) -> str:
         return f"sC[{self.idx[sp]}][t]"
 
     def E(self, sp: str) -> str:
+        if self.tmem:
+            return self._eloc[sp]
         return f"sE[{self.idx[sp]}][t]"
+
+    def tmem_cols(self) -> int:
+        """Tensor-memory columns the FP64 kernel allocates (a power of two)."""
+        need = -(-self.block // 128) * 2 * self.ns
+        n = 32
+        while n < need:
+            n *= 2
+        return n
+
+    def load_egp(self, r: Reaction) -> List[str]:
+        """Tensor-memory mode: load the reaction's EGp values into locals, in
+        batches of up to four loads that share one wait."""
+        sps = list(dict.fromkeys(list(r.reactants) + list(r.products)))
+        self._eloc = {sp: f"e{j}" for j, sp in enumerate(sps)}
+        L = ["double " + ", ".join(self._eloc[sp] for sp in sps) + ";"]
+        for b in range(0, len(sps), 4):
+            grp = sps[b:b + 4]
+            addrs = ", ".join(f"tw + {2 * self.idx[sp]}u" for sp in grp)
+            outs = ", ".join(self._eloc[sp] for sp in grp)
+            L.append(f"cgg::tm_ld({addrs}, {outs});")
+        return L
 
     def W(self, sp: str) -> str:
         k = self.idx[sp]
@@ -231,6 +259,8 @@ class _Emitter:
             body += self.falloff64(r)
         qf = f"kf*{self.prod(r.reactants, self.C)}"
         if r.reversible:
+            if self.tmem:
+                body += self.load_egp(r)
             num = self.prod(r.reactants, self.E)
             den = self.prod(r.products, self.E)
             body.append(f"const double rr = {qf} - kf*({num})*rcp({den})*{self.prod(r.products, self.C)};")
@@ -416,9 +446,14 @@ class _Emitter:
                     vals.append(c[0] + c[1] * math.log(t) + c[2] * t + c[3] * t * t + c[4] * t ** 3
                                 + c[5] * t ** 4 - c[6] / t)
                 fn = "cgm::cg_exp" if max(abs(v) for v in vals) < 690.0 else "cgm::cg_exp_clamped"
-                L.append(f"{{ {pre}sE[{k}][t] = {fn}({poly}) * pfac; }}")
+                if self.tmem:
+                    L.append(f"{{ {pre}cgg::tm_st(tw + {2 * k}u, {fn}({poly}) * pfac); }}")
+                else:
+                    L.append(f"{{ {pre}sE[{k}][t] = {fn}({poly}) * pfac; }}")
             else:
                 L.append(f"{{ {pre}sG[{k}][t] = fma({poly}, {_d(LOG2E)}, lpfac2); }}")
+        if self.tmem and not mixed:
+            L.append("cgg::tm_wait_st();")
         if self.reg_w:
             L.append("double " + ", ".join(f"w{k} = 0.0" for k in range(ns)) + ";")
         else:
@@ -435,7 +470,7 @@ class _Emitter:
         return L
 
     def smem_bytes(self, mixed: bool) -> int:
-        per = (16 if not mixed else 12) + (0 if self.reg_w else 8)
+        per = (12 if mixed else (8 if self.tmem else 16)) + (0 if self.reg_w else 8)
         return per * self.ns * self.block
 
     def kernel(self, mixed: bool) -> str:
@@ -445,7 +480,13 @@ class _Emitter:
              "const double* __restrict__ T, const double* __restrict__ Y, double* __restrict__ wdot, int64_t ng) {"]
         # dynamic shared memory: [array][species][thread]
         L.append("  extern __shared__ __align__(16) unsigned char dsm[];")
-        if not mixed:
+        if not mixed and self.tmem:
+            L.append(f"  double (*sC)[{B}] = reinterpret_cast<double (*)[{B}]>(dsm);")
+            L.append("  __shared__ uint32_t tm_slot;")
+            L.append(f"  const uint32_t tbase = cgg::tm_alloc(&tm_slot, {self.tmem_cols()}u);")
+            L.append(f"  const uint32_t tw = cgg::tm_thread_base(tbase, {2 * ns});")
+            off = ns * B * 8
+        elif not mixed:
             L.append(f"  double (*sC)[{B}] = reinterpret_cast<double (*)[{B}]>(dsm);")
             L.append(f"  double (*sE)[{B}] = reinterpret_cast<double (*)[{B}]>(dsm + {ns * B * 8});")
             off = 2 * ns * B * 8
@@ -463,22 +504,43 @@ class _Emitter:
                 L.append("  __syncthreads();")
             L += ["  " + x for x in (self.reaction32(r) if mixed else self.reaction64(r))]
         L += ["  " + x for x in self.epilogue()]
+        if not mixed and self.tmem:
+            L.append(f"  cgg::tm_free(tbase, {self.tmem_cols()}u);")
         L.append("}")
         return "\n".join(L)
 
 
-def choose_block(ns: int) -> int:
-    """One 256-thread block per SM when the per-point state fits (all warps of
-    the SM then walk the code together), else 128."""
-    per = 16 * ns
-    return 256 if 256 * per <= SMEM_BUDGET else 128
+def choose_block(ns: int, mixed: bool, tmem: bool = False) -> int:
+    """Threads per block; one block per SM, so this is also the SM's resident
+    points.  The straight-line kernels are latency-bound: resident warps pay
+    off until the per-point shared-memory state or the registers (two per
+    FP64 accumulator plus ~64 temporaries) run out.  Measured on B200: 53/325
+    mixed 8 -> 11 warps 624 -> 770 Mpts/s; 24/325 FP64 8 -> 16 warps
+    450 -> 850 Mpts/s; 16 warps at 53 species spill and lose the gain."""
+    reg_w = ns <= MAX_REG_SPECIES
+    per = ((12 if mixed else (8 if tmem else 16)) + (0 if reg_w else 8)) * ns
+    regs = (2 * ns if reg_w else 0) + 64
+    b = min(SMEM_BUDGET // per, REG_FILE // regs, MAX_BLOCK) // 32 * 32
+    if tmem:
+        while b > 32 and -(-b // 128) * 2 * ns > 512:     # 512 tensor-memory columns per SM
+            b -= 32
+    return max(b, 32)
+
+
+def use_tmem(ns: int) -> bool:
+    """FP64 kernel: EGp moves to tensor memory when that lets the block grow
+    (shared memory, not registers, limits it) and the columns fit."""
+    if ns > MAX_REG_SPECIES:
+        return False
+    b = choose_block(ns, False, True)
+    return b > choose_block(ns, False) and -(-b // 128) * 2 * ns <= 512
 
 
 PRECISIONS = {"fp64": (True, False), "mixed": (False, True), "both": (True, True)}
 
 
 def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = None,
-         sync_every: int = SYNC_EVERY, precision: str = "both") -> str:
+         sync_every: int = SYNC_EVERY, precision: str = "both", tmem: Optional[bool] = None) -> str:
     """CUDA source of the mechanism's kernels: `precision` selects the FP64
     kernel, the mixed one or both; a mode without a generated kernel runs on
     the table-driven kernels."""
@@ -487,8 +549,9 @@ def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = Non
     want64, want32 = PRECISIONS[precision]
     blob = pack(mech).to_blob()
     fp = fingerprint(blob)
-    block = block or choose_block(mech.ns)
-    em = _Emitter(mech, block, sync_every)
+    tm = use_tmem(mech.ns) if tmem is None else tmem
+    em64 = _Emitter(mech, block or choose_block(mech.ns, False, tm), sync_every, tmem=tm)
+    em32 = _Emitter(mech, block or choose_block(mech.ns, True), sync_every)
     ident = "".join(ch if ch.isalnum() else "_" for ch in (name or mech.name))
     src = [
         f"// Generated by chemgen_b200 (generate_chemistry.py --language cuda --precision {precision}) for mechanism '{mech.name}':",
@@ -500,17 +563,16 @@ def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = Non
         "namespace {",
     ]
     attrs, dispatch = [], []
-    if want64:
-        src += [em.kernel(False), ""]
-        attrs.append(f"cudaFuncSetAttribute(cg_gen_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, "
-                     f"{em.smem_bytes(False)}) != cudaSuccess")
-        dispatch.append(f"  if (mode == CHEMGEN_MODE_FP64) {{ cg_gen_fp64<<<blocks, {block}, {em.smem_bytes(False)}, st>>>"
-                        "(P, T, Y, wdot, ng); return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA; }")
-    if want32:
-        src += [em.kernel(True), ""]
-        attrs.append(f"cudaFuncSetAttribute(cg_gen_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, "
-                     f"{em.smem_bytes(True)}) != cudaSuccess")
-        dispatch.append(f"  if (mode == CHEMGEN_MODE_MIXED) {{ cg_gen_mixed<<<blocks, {block}, {em.smem_bytes(True)}, st>>>"
+    for want, em, mixed, kname, mname in ((want64, em64, False, "cg_gen_fp64", "CHEMGEN_MODE_FP64"),
+                                          (want32, em32, True, "cg_gen_mixed", "CHEMGEN_MODE_MIXED")):
+        if not want:
+            continue
+        B = em.block
+        src += [em.kernel(mixed), ""]
+        attrs.append(f"cudaFuncSetAttribute({kname}, cudaFuncAttributeMaxDynamicSharedMemorySize, "
+                     f"{em.smem_bytes(mixed)}) != cudaSuccess")
+        dispatch.append(f"  if (mode == {mname}) {{ {kname}<<<(unsigned)((ng + {B - 1}) / {B}), {B}, "
+                        f"{em.smem_bytes(mixed)}, st>>>"
                         "(P, T, Y, wdot, ng); return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA; }")
     modes = (1 if want64 else 0) | (2 if want32 else 0)
     src += [
@@ -522,7 +584,6 @@ def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = Non
         "      return CHEMGEN_ERR_CUDA;",
         "    attrs = true;",
         "  }",
-        f"  const unsigned blocks = (unsigned)((ng + {block - 1}) / {block});",
         "  cudaStream_t st = (cudaStream_t)s;",
     ] + dispatch + [
         "  return CHEMGEN_ERR_INVALID_ARGUMENT;",
