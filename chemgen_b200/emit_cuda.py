@@ -32,7 +32,8 @@ LOG10_2 = 0.30102999566398119521
 CSCALE_LOG2 = 32          # mixed: concentrations are stored as C * 2^32 in FP32
 # register-resident wdot accumulators up to this many species
 MAX_REG_SPECIES = 72
-SYNC_EVERY = 48           # reactions between block barriers (B200 sweep at 53/325: 2..64, best 48-64)
+SYNC_EVERY = 48           # reactions between block barriers, FP64 kernel (B200 sweep at 53/325: 2..64)
+SYNC_EVERY_MIXED = 24     # mixed kernel (B200 sweep at 53/325: 16..96, best 24-48)
 SMEM_BUDGET = 220 * 1024  # dynamic shared memory per block
 REG_FILE = 65536          # 32-bit registers per SM
 MAX_BLOCK = 512           # 16 warps; beyond this the 53-species kernels spill heavily
@@ -69,7 +70,8 @@ class _Emitter:
         self.block = block
         self.reg_w = self.ns <= MAX_REG_SPECIES
         self.has_m = any(r.uses_m for r in mech.reactions)
-        # FP64 kernel only: EGp in tensor memory instead of shared memory
+        # EGp (FP64 kernel) or the log2 Gibbs terms (mixed) in tensor memory
+        # instead of shared memory
         self.tmem = tmem
         self._eloc: Dict[str, str] = {}
 
@@ -82,6 +84,11 @@ class _Emitter:
             return self._eloc[sp]
         return f"sE[{self.idx[sp]}][t]"
 
+    def G(self, sp: str) -> str:
+        if self.tmem:
+            return self._eloc[sp]
+        return f"sG[{self.idx[sp]}][t]"
+
     def tmem_cols(self) -> int:
         """Tensor-memory columns the FP64 kernel allocates (a power of two)."""
         need = -(-self.block // 128) * 2 * self.ns
@@ -91,8 +98,9 @@ class _Emitter:
         return n
 
     def load_egp(self, r: Reaction) -> List[str]:
-        """Tensor-memory mode: load the reaction's EGp values into locals, in
-        batches of up to four loads that share one wait."""
+        """Tensor-memory mode: load the reaction's EGp (FP64 kernel) or log2
+        Gibbs values (mixed) into locals, in batches of up to four loads that
+        share one wait."""
         sps = list(dict.fromkeys(list(r.reactants) + list(r.products)))
         self._eloc = {sp: f"e{j}" for j, sp in enumerate(sps)}
         L = ["double " + ", ".join(self._eloc[sp] for sp in sps) + ";"]
@@ -289,7 +297,7 @@ class _Emitter:
         terms = [(nu, sp) for sp, nu in r.reactants.items()] + [(-nu, sp) for sp, nu in r.products.items()]
         expr = None
         for coef, sp in terms:
-            g = f"sG[{self.idx[sp]}][t]"
+            g = self.G(sp)
             if expr is None:
                 expr = g if coef == 1.0 else f"{_d(coef)}*{g}"
             elif coef == 1.0:
@@ -363,6 +371,8 @@ class _Emitter:
             sgn = ""
         body.append(f"double rr = {sgn}cgg::rate2(akf, {cf}, {-CSCALE_LOG2 * of});")
         if r.reversible:
+            if self.tmem:
+                body += self.load_egp(r)
             body.append(f"rr -= {sgn}cgg::rate2(akf + {self.gsum(r)}, {cb}, {-CSCALE_LOG2 * ob});")
         body += self.scatter(r, "rr")
         L += ["  " + x for x in body] + ["}"]
@@ -373,7 +383,7 @@ class _Emitter:
         L = [f"{{ // {r.equation} (FP64)"]
         body = []
         C = lambda sp: f"((double)sc[{self.idx[sp]}][t] * {_d(2.0 ** -CSCALE_LOG2)})"
-        E = lambda sp: f"exp2(sG[{self.idx[sp]}][t])"
+        E = lambda sp: f"exp2({self.G(sp)})"
         if r.uses_m:
             m = "((double)ctot32 * " + _d(2.0 ** -CSCALE_LOG2) + ")"
             for sp, e in r.efficiencies.items():
@@ -387,6 +397,8 @@ class _Emitter:
             body += self.falloff64(r)
         qf = f"kf*{self.prod(r.reactants, C)}"
         if r.reversible:
+            if self.tmem:
+                body += self.load_egp(r)
             body.append(f"const double rr = {qf} - kf*({self.prod(r.reactants, E)})*rcp({self.prod(r.products, E)})"
                         f"*{self.prod(r.products, C)};")
         else:
@@ -410,11 +422,17 @@ class _Emitter:
         if any(r.kind == "plog" for r in self.mech.reactions):
             L.append("const double lnP = cgm::cg_log(Pv);")
         mw = self.mech.mw()
-        tmp = "sC" if not mixed else "sG"          # unscaled Y/W, overwritten below
         L.append("double csum = 0.0;")
-        for k in range(ns):
-            L.append(f"{{ const double c = (act ? Y[(int64_t){k} * ng + i] : 1.0) * {_d(1.0 / r15(mw[k]))}; "
-                     f"{tmp}[{k}][t] = c; csum += c; }}")
+        if mixed and self.tmem:
+            # unscaled Y/W in registers (the accumulators are not live yet)
+            for k in range(ns):
+                L.append(f"const double y{k} = (act ? Y[(int64_t){k} * ng + i] : 1.0) * {_d(1.0 / r15(mw[k]))}; "
+                         f"csum += y{k};")
+        else:
+            tmp = "sC" if not mixed else "sG"      # unscaled Y/W, overwritten below
+            for k in range(ns):
+                L.append(f"{{ const double c = (act ? Y[(int64_t){k} * ng + i] : 1.0) * {_d(1.0 / r15(mw[k]))}; "
+                         f"{tmp}[{k}][t] = c; csum += c; }}")
         L.append(f"const double fac = Pv * rcp({_d(8.314510e+07)} * csum * Tv);")
         L.append("double ctot = 0.0;")
         if not mixed:
@@ -424,7 +442,8 @@ class _Emitter:
         else:
             L.append(f"const double facs = fac * {_d(2.0 ** CSCALE_LOG2)};")
             for k in range(ns):
-                L.append(f"{{ const double c = sG[{k}][t] * facs; sc[{k}][t] = (float)c; ctot += c; }}")
+                src = f"y{k}" if self.tmem else f"sG[{k}][t]"
+                L.append(f"{{ const double c = {src} * facs; sc[{k}][t] = (float)c; ctot += c; }}")
             L.append("const float ctot32 = (float)ctot;")
             L.append(f"const double lnT2 = lnT * {_d(LOG2E)};")
             L.append(f"const double lpfac2 = {_d(math.log2(1013250.0 / 8.314510e+07))} - lnT2;")
@@ -451,8 +470,11 @@ class _Emitter:
                 else:
                     L.append(f"{{ {pre}sE[{k}][t] = {fn}({poly}) * pfac; }}")
             else:
-                L.append(f"{{ {pre}sG[{k}][t] = fma({poly}, {_d(LOG2E)}, lpfac2); }}")
-        if self.tmem and not mixed:
+                if self.tmem:
+                    L.append(f"{{ {pre}cgg::tm_st(tw + {2 * k}u, fma({poly}, {_d(LOG2E)}, lpfac2)); }}")
+                else:
+                    L.append(f"{{ {pre}sG[{k}][t] = fma({poly}, {_d(LOG2E)}, lpfac2); }}")
+        if self.tmem:
             L.append("cgg::tm_wait_st();")
         if self.reg_w:
             L.append("double " + ", ".join(f"w{k} = 0.0" for k in range(ns)) + ";")
@@ -470,8 +492,7 @@ class _Emitter:
         return L
 
     def smem_bytes(self, mixed: bool) -> int:
-        per = (12 if mixed else (8 if self.tmem else 16)) + (0 if self.reg_w else 8)
-        return per * self.ns * self.block
+        return smem_per_species(mixed, self.tmem, self.reg_w) * self.ns * self.block
 
     def kernel(self, mixed: bool) -> str:
         ns, B = self.ns, self.block
@@ -490,6 +511,12 @@ class _Emitter:
             L.append(f"  double (*sC)[{B}] = reinterpret_cast<double (*)[{B}]>(dsm);")
             L.append(f"  double (*sE)[{B}] = reinterpret_cast<double (*)[{B}]>(dsm + {ns * B * 8});")
             off = 2 * ns * B * 8
+        elif self.tmem:
+            L.append(f"  float (*sc)[{B}] = reinterpret_cast<float (*)[{B}]>(dsm);")
+            L.append("  __shared__ uint32_t tm_slot;")
+            L.append(f"  const uint32_t tbase = cgg::tm_alloc(&tm_slot, {self.tmem_cols()}u);")
+            L.append(f"  const uint32_t tw = cgg::tm_thread_base(tbase, {2 * ns});")
+            off = ns * B * 4
         else:
             L.append(f"  double (*sG)[{B}] = reinterpret_cast<double (*)[{B}]>(dsm);")
             L.append(f"  float (*sc)[{B}] = reinterpret_cast<float (*)[{B}]>(dsm + {ns * B * 8});")
@@ -504,22 +531,33 @@ class _Emitter:
                 L.append("  __syncthreads();")
             L += ["  " + x for x in (self.reaction32(r) if mixed else self.reaction64(r))]
         L += ["  " + x for x in self.epilogue()]
-        if not mixed and self.tmem:
+        if self.tmem:
             L.append(f"  cgg::tm_free(tbase, {self.tmem_cols()}u);")
         L.append("}")
         return "\n".join(L)
 
 
+def smem_per_species(mixed: bool, tmem: bool, reg_w: bool) -> int:
+    """Shared-memory bytes per species and point: C (FP64) and EGp, or, for
+    the mixed kernel, C (FP32) and the log2 Gibbs terms (FP64); the second
+    array leaves for tensor memory in tmem mode; wdot when not in registers."""
+    per = (4 if tmem else 12) if mixed else (8 if tmem else 16)
+    return per + (0 if reg_w else 8)
+
+
 def choose_block(ns: int, mixed: bool, tmem: bool = False) -> int:
     """Threads per block; one block per SM, so this is also the SM's resident
     points.  The straight-line kernels are latency-bound: resident warps pay
-    off until the per-point shared-memory state or the registers (two per
-    FP64 accumulator plus ~64 temporaries) run out.  Measured on B200: 53/325
-    mixed 8 -> 11 warps 624 -> 770 Mpts/s; 24/325 FP64 8 -> 16 warps
-    450 -> 850 Mpts/s; 16 warps at 53 species spill and lose the gain."""
+    off until the per-point state (shared and tensor memory) or the registers
+    run out.  Registers: two per FP64 accumulator plus temporaries (~64 when
+    the Gibbs array is in shared memory, whose loads the compiler hoists;
+    ~20 when batched tensor-memory loads replace them).  Measured on B200 at
+    53/325: FP64 8 warps 394, 12 warps (tensor memory) 468, 16 warps 510
+    Mpts/s; mixed 8 warps 624, 11 warps 775 Mpts/s; at 24/325 FP64 8 -> 16
+    warps 450 -> 850 Mpts/s."""
     reg_w = ns <= MAX_REG_SPECIES
-    per = ((12 if mixed else (8 if tmem else 16)) + (0 if reg_w else 8)) * ns
-    regs = (2 * ns if reg_w else 0) + 64
+    per = smem_per_species(mixed, tmem, reg_w) * ns
+    regs = (2 * ns if reg_w else 0) + (20 if tmem else 64)
     b = min(SMEM_BUDGET // per, REG_FILE // regs, MAX_BLOCK) // 32 * 32
     if tmem:
         while b > 32 and -(-b // 128) * 2 * ns > 512:     # 512 tensor-memory columns per SM
@@ -527,20 +565,24 @@ def choose_block(ns: int, mixed: bool, tmem: bool = False) -> int:
     return max(b, 32)
 
 
-def use_tmem(ns: int) -> bool:
+def use_tmem(ns: int, mixed: bool = False) -> bool:
     """FP64 kernel: EGp moves to tensor memory when that lets the block grow
-    (shared memory, not registers, limits it) and the columns fit."""
-    if ns > MAX_REG_SPECIES:
+    and the columns fit.  The mixed kernel keeps its Gibbs terms in shared
+    memory by default: at 53/325 the tensor-memory form (16 warps, 761-770
+    Mpts/s on B200) lost to 11 warps in shared memory (795 Mpts/s), its extra
+    load instructions outweighing the extra warps; emit(tmem=True) still
+    selects it."""
+    if ns > MAX_REG_SPECIES or mixed:
         return False
-    b = choose_block(ns, False, True)
-    return b > choose_block(ns, False) and -(-b // 128) * 2 * ns <= 512
+    b = choose_block(ns, mixed, True)
+    return b > choose_block(ns, mixed) and -(-b // 128) * 2 * ns <= 512
 
 
 PRECISIONS = {"fp64": (True, False), "mixed": (False, True), "both": (True, True)}
 
 
 def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = None,
-         sync_every: int = SYNC_EVERY, precision: str = "both", tmem: Optional[bool] = None) -> str:
+         sync_every: Optional[int] = None, precision: str = "both", tmem: Optional[bool] = None) -> str:
     """CUDA source of the mechanism's kernels: `precision` selects the FP64
     kernel, the mixed one or both; a mode without a generated kernel runs on
     the table-driven kernels."""
@@ -549,9 +591,12 @@ def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = Non
     want64, want32 = PRECISIONS[precision]
     blob = pack(mech).to_blob()
     fp = fingerprint(blob)
-    tm = use_tmem(mech.ns) if tmem is None else tmem
-    em64 = _Emitter(mech, block or choose_block(mech.ns, False, tm), sync_every, tmem=tm)
-    em32 = _Emitter(mech, block or choose_block(mech.ns, True), sync_every)
+    tm64 = use_tmem(mech.ns, False) if tmem is None else tmem
+    tm32 = use_tmem(mech.ns, True) if tmem is None else tmem
+    em64 = _Emitter(mech, block or choose_block(mech.ns, False, tm64),
+                    SYNC_EVERY if sync_every is None else sync_every, tmem=tm64)
+    em32 = _Emitter(mech, block or choose_block(mech.ns, True, tm32),
+                    SYNC_EVERY_MIXED if sync_every is None else sync_every, tmem=tm32)
     ident = "".join(ch if ch.isalnum() else "_" for ch in (name or mech.name))
     src = [
         f"// Generated by chemgen_b200 (generate_chemistry.py --language cuda --precision {precision}) for mechanism '{mech.name}':",
