@@ -3,8 +3,9 @@
 //
 // A generated kernel handles one grid point per thread.  Species indices,
 // stoichiometry and coefficients are compile-time constants; the wdot
-// accumulators are registers; C and EGp = exp(smh) * Patm/(R0 T) (FP64) or the
-// log2 Gibbs terms (mixed) live in shared memory as [species][thread].
+// accumulators are registers; C lives in shared memory as [species][thread],
+// and EGp = exp(smh) * Patm/(R0 T) (FP64) or the log2 Gibbs terms (mixed)
+// either beside it or, when that lets the block grow, in tensor memory.
 #pragma once
 
 #include <cstdint>
@@ -91,8 +92,9 @@ __device__ __forceinline__ double rate2(double a, float prod, int eoff) {
 
 // ------------------------------------------------------- tensor memory
 // When shared memory cannot hold both per-point arrays for the block size
-// the kernel wants, the FP64 kernel keeps EGp in tensor memory instead: each
-// thread owns one lane (warp w reaches lanes 32 (w % 4) .. 32 (w % 4) + 31)
+// the kernel wants, the FP64 kernel keeps EGp in tensor memory instead (the
+// mixed kernel can do the same with its log2 Gibbs terms): each thread owns
+// one lane (warp w reaches lanes 32 (w % 4) .. 32 (w % 4) + 31)
 // and, for warp slot w / 4, 2 ns consecutive 32-bit columns, species k at
 // columns 2k, 2k+1 (low, high word).  The tcgen05 ld/st are warp-collective;
 // the generated kernels call them from straight-line code that every thread
