@@ -46,7 +46,8 @@ constexpr uint32_t kABytes = kPts * kHid * 2;                // hidden activatio
 constexpr uint32_t kFBytes = kPts * kK1 * 2;                 // features, K = 128
 constexpr uint32_t kWBytes = kHid * kHid * 2;
 constexpr uint32_t kFOff = kABytes, kWOff = kFOff + kFBytes, kTailOff = kWOff + kWBytes;
-constexpr size_t kSmem = (size_t)kTailOff + 64;             // 4 mbarriers, TMEM slot, flags
+constexpr uint32_t kOobOff = kTailOff + 64;                 // out-of-range flags, [tile parity][row]
+constexpr size_t kSmem = (size_t)kOobOff + 2 * kPts;         // + 4 mbarriers, TMEM slot, fail words
 constexpr uint32_t kCopyPiece = 16384;
 
 __device__ int g_sur_err;
@@ -97,18 +98,33 @@ __device__ __forceinline__ void issue_weights(const bf16* img, int l, unsigned c
 // Feature group: the 64 inputs of point `row` of `tile`, as BF16 hi/lo parts
 // into sF (K = 128 canonical layout).  All loads use clamped (valid) indices
 // so that they are in flight together; absent points and padding give 0.
-__device__ __forceinline__ void write_features(unsigned char* sF, int row, int64_t tile, int64_t ng, int ns,
+// Returns whether the point lies outside the training support given by
+// `range` (T in [range[0], range[1]], P in [range[2], range[3]], every Y_k
+// >= 0 and |sum Y - 1| < 1e-6; NaN fails); no range, no check.
+__device__ __forceinline__ bool write_features(unsigned char* sF, int row, int64_t tile, int64_t ng, int ns,
                                                const double* __restrict__ P, const double* __restrict__ T,
                                                const double* __restrict__ Y, const double* __restrict__ inv_mw,
-                                               const float* nrm) {
+                                               const float* nrm, const double* __restrict__ range) {
     const int64_t i = tile * kPts + row;
     const bool act = i < ng;
     const int64_t ic = act ? i : ng - 1;
     float y[kDin - 3];
+    double ysum = 0.0, ymin = 0.0;
 #pragma unroll
-    for (int k = 0; k < kDin - 3; ++k) y[k] = (float)__ldg(Y + (int64_t)min(k, ns - 1) * ng + ic);
-    const double t = __ldg(T + ic);
-    const float invT = (float)(1000.0 / t), lnT = logf((float)t), lnP = logf((float)(__ldg(P + ic) / 1013250.0));
+    for (int k = 0; k < kDin - 3; ++k) {
+        const double yd = __ldg(Y + (int64_t)min(k, ns - 1) * ng + ic);
+        y[k] = (float)yd;
+        if (k < ns) {
+            ysum += yd;
+            ymin = fmin(ymin, yd);
+        }
+    }
+    const double t = __ldg(T + ic), pr = __ldg(P + ic);
+    bool oob = false;
+    if (range && act)
+        oob = !(t >= __ldg(range) && t <= __ldg(range + 1) && pr >= __ldg(range + 2) && pr <= __ldg(range + 3) &&
+                ymin >= 0.0 && fabs(ysum - 1.0) < 1e-6);
+    const float invT = (float)(1000.0 / t), lnT = logf((float)t), lnP = logf((float)(pr / 1013250.0));
     float mix = 0.0f;
 #pragma unroll
     for (int k = 0; k < kDin - 3; ++k)
@@ -148,6 +164,7 @@ __device__ __forceinline__ void write_features(unsigned char* sF, int row, int64
         *reinterpret_cast<uint4*>(sF + um::kmajor_offset(row, kDin + 8 * g, kK1)) =
             make_uint4(lo[0], lo[1], lo[2], lo[3]);
     }
+    return oob;
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
@@ -155,7 +172,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                            const float* __restrict__ norm, const float* __restrict__ lnorm,
                            const double* __restrict__ inv_mw, int ns, const double* __restrict__ P,
                            const double* __restrict__ T, const double* __restrict__ Y, int64_t ng,
-                           double* __restrict__ W, float* __restrict__ est) {
+                           double* __restrict__ W, float* __restrict__ est, const double* __restrict__ range) {
     extern __shared__ __align__(1024) unsigned char sm[];
     unsigned char* sA = sm;
     unsigned char* sF = sm + kFOff;
@@ -166,6 +183,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     volatile int* wfail = reinterpret_cast<volatile int*>(tslot + 1);   // set by thread 0 before a barrier
     volatile int* mfail = wfail + 1;                                     // set after the MMA wait
     volatile int* ffail = wfail + 2;                                     // feature group gave up
+    // out-of-range flag of each row, one slot per tile parity: the feature
+    // group writes tile j's before "features full" of tile j and tile j+2's
+    // only after "features empty" of tile j+1, which the compute group
+    // signals after the decode of tile j has read them
+    unsigned char* sOob = sm + kOobOff;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int64_t ntiles = (ng + kPts - 1) / kPts;
     if (tid == 0) {
@@ -208,7 +230,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) um::bulk_prefetch_l2(src, bytes);
                 }
             }
-            write_features(sF, row, tile, ng, ns, P, T, Y, inv_mw, nrm);
+            sOob[(j & 1) * kPts + row] = write_features(sF, row, tile, ng, ns, P, T, Y, inv_mw, nrm, range);
             um::fence_proxy_async();
             um::mbar_arrive(&bars[2]);
         }
@@ -282,6 +304,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         const float* b4 = bias + 3 * kHid;
                         const int64_t i = tile * kPts + erow;
                         const bool act = i < ng;
+                        const bool oob = sOob[(j & 1) * kPts + erow] != 0;
                         const int cL = (ns / 16) * 16;
                         float v[16];
                         um::tmem_ld16(um::tmem_lane_addr(tbase, g4, cL), v);
@@ -298,7 +321,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                                 for (int q = 0; q < 16; ++q) {
                                     const int k = c + q;
                                     if (k < ns) W[(int64_t)k * ng + i] = (double)(v[q] + __ldg(b4 + k)) * scale;
-                                    else if (k == ns + 1 && est) est[i] = v[q] + __ldg(b4 + k);
+                                    else if (k == ns + 1 && est) est[i] = oob ? INFINITY : v[q] + __ldg(b4 + k);
                                 }
                             }
                         }
@@ -374,7 +397,7 @@ int chemgen_surrogate_pack(const void* W1, const void* W2, const void* W3, const
 
 int chemgen_surrogate_infer(const void* img, const float* bias, const float* norm, const float* lnorm,
                             const double* inv_mw, int ns, const double* P, const double* T, int64_t ng,
-                            const double* Y, double* wdot, float* err_est, void* stream) {
+                            const double* Y, double* wdot, float* err_est, const double* range, void* stream) {
     if (!img || !bias || !norm || !lnorm || !inv_mw || !P || !T || !Y || !wdot || ng < 0)
         return CHEMGEN_ERR_INVALID_ARGUMENT;
     if (ns < 1 || ns + 3 > kDin || ns + 2 > kDout) return CHEMGEN_ERR_UNSUPPORTED;
@@ -392,7 +415,7 @@ int chemgen_surrogate_infer(const void* img, const float* bias, const float* nor
     const int64_t ntiles = (ng + kPts - 1) / kPts;
     const unsigned grid = (unsigned)(ntiles < sms ? ntiles : sms);
     surrogate_infer_kernel<<<grid, kThreads, kSmem, (cudaStream_t)stream>>>(
-        (const bf16*)img, bias, norm, lnorm, inv_mw, ns, P, T, Y, ng, wdot, err_est);
+        (const bf16*)img, bias, norm, lnorm, inv_mw, ns, P, T, Y, ng, wdot, err_est, range);
     return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA;
 }
 

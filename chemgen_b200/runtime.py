@@ -79,7 +79,7 @@ def lib() -> ctypes.CDLL:
     L.chemgen_surrogate_decode.argtypes = [vp, i64, ci, ci, vp, vp, vp, vp]
     L.chemgen_surrogate_image_elems.argtypes = []
     L.chemgen_surrogate_pack.argtypes = [vp, vp, vp, vp, vp, vp]
-    L.chemgen_surrogate_infer.argtypes = [vp, vp, vp, vp, vp, ci, vp, vp, i64, vp, vp, vp, vp]
+    L.chemgen_surrogate_infer.argtypes = [vp, vp, vp, vp, vp, ci, vp, vp, i64, vp, vp, vp, vp, vp]
     L.chemgen_surrogate_infer_error.argtypes = [ci]
     for f in ("chemgen_mlp_gemm", "chemgen_mlp_bias_gelu", "chemgen_mlp_gelu_backward", "chemgen_mlp_mse_grad",
               "chemgen_mlp_colsum", "chemgen_mlp_adam", "chemgen_surrogate_features", "chemgen_surrogate_targets",

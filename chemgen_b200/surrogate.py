@@ -445,27 +445,42 @@ class Surrogate:
             self._img = (img, torch.cat(self.net.b).contiguous())
         return self._img
 
-    def predict_fused(self, P, T, Y, out=None, est=None):
+    def range_bounds(self):
+        """Device copy of the training support {T_lo, T_hi, P_lo, P_hi} (P
+        widened by 0.1 %) that the fused kernel checks."""
+        import torch
+        key = (self.T_range, self.P_range)
+        if getattr(self, "_range_key", None) != key:
+            self._range_dev = torch.tensor([self.T_range[0], self.T_range[1], self.P_range[0] * 0.999,
+                                            self.P_range[1] * 1.001], dtype=torch.float64, device=self.dev)
+            self._range_key = key
+        return self._range_dev
+
+    def predict_fused(self, P, T, Y, out=None, est=None, check_range: bool = False):
         """(wdot [ns, ng] FP64, log10 error estimate [ng]) from the fused
-        tensor-core kernel (one launch)."""
+        tensor-core kernel (one launch); with `check_range` the kernel sets
+        the estimate of points outside the training support to +inf."""
         import torch
         ng = T.numel()
         img, bias = self.packed()
         W = out if out is not None else torch.empty((self.ns, ng), dtype=torch.float64, device=self.dev)
         e = est if est is not None else torch.empty(ng, dtype=torch.float32, device=self.dev)
+        rng = self.range_bounds().data_ptr() if check_range else None
         check(lib().chemgen_surrogate_infer(img.data_ptr(), bias.data_ptr(), self.norm.data_ptr(),
                                             self.lnorm.data_ptr(), self.inv_mw.data_ptr(), self.ns, P.data_ptr(),
-                                            T.data_ptr(), ng, Y.data_ptr(), W.data_ptr(), e.data_ptr(), _stream()),
+                                            T.data_ptr(), ng, Y.data_ptr(), W.data_ptr(), e.data_ptr(), rng,
+                                            _stream()),
               "surrogate_infer")
         return W, e
 
-    def predict(self, P, T, Y, chunk: int = 1 << 20, fused: bool = True):
+    def predict(self, P, T, Y, chunk: int = 1 << 20, fused: bool = True, check_range: bool = False):
         """(wdot [ns, ng] FP64, log10 error estimate [ng]); `fused` selects
         the one-kernel tensor-core path, otherwise the layer-by-layer kernels
-        used in training."""
+        used in training.  With `check_range`, points outside the training
+        support (`in_range`) get an error estimate of +inf."""
         import torch
         if fused:
-            return self.predict_fused(P.contiguous(), T.contiguous(), Y.contiguous())
+            return self.predict_fused(P.contiguous(), T.contiguous(), Y.contiguous(), check_range=check_range)
         ng = T.numel()
         W = torch.empty((self.ns, ng), dtype=torch.float64, device=self.dev)
         est = torch.empty(ng, dtype=torch.float32, device=self.dev)
@@ -476,6 +491,8 @@ class Surrogate:
             w, e = self.decode(out)
             W[:, i0:i1] = w
             est[i0:i1] = e
+        if check_range:
+            est.masked_fill_(~self.in_range(P, T, Y), math.inf)
         return W, est
 
     def in_range(self, P, T, Y):
@@ -497,8 +514,9 @@ class SurrogateGetrates:
 
     def __call__(self, P, T, Y):
         import torch
-        W, est = self.sur.predict(P, T, Y)
-        ok = self.sur.in_range(P, T, Y) & (est <= math.log10(self.tol))
+        # the fused kernel folds the training-support check into the estimate
+        W, est = self.sur.predict(P, T, Y, check_range=True)
+        ok = est <= math.log10(self.tol)
         bad = torch.nonzero(~ok).flatten()
         if bad.numel():
             Pb, Tb = P.index_select(0, bad).contiguous(), T.index_select(0, bad).contiguous()

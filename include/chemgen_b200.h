@@ -157,14 +157,16 @@ int chemgen_surrogate_decode(const float* out, int64_t ng, int ns, int dout, con
  *   operands in the tensor cores' K-major canonical layout, layer 1 with its input weights twice.
  * chemgen_surrogate_infer: wdot[k*ng + i] and err_est[i] (may be NULL) from (P, T, Y) with bias =
  *   (b1, b2, b3 [256 each], b4 [64]), norm[8], lnorm[2] and inv_mw[ns] as in
- *   chemgen_surrogate_features / _decode.  Asynchronous on `stream`.
+ *   chemgen_surrogate_features / _decode.  range (device, may be NULL) = {T_lo, T_hi, P_lo, P_hi}:
+ *   a point with T or P outside it, a negative Y_k, |sum Y - 1| >= 1e-6 or a NaN gets
+ *   err_est = +inf, so that an error gate sends it to the exact kernel.  Asynchronous on `stream`.
  * chemgen_surrogate_infer_error: 1 if a bounded wait inside the kernel ever gave up (its outputs
  *   are then incomplete), 0 otherwise, -1 on a CUDA error; synchronous; reset != 0 clears it. */
 int chemgen_surrogate_image_elems(void);
 int chemgen_surrogate_pack(const void* W1, const void* W2, const void* W3, const void* W4, void* img, void* stream);
 int chemgen_surrogate_infer(const void* img, const float* bias, const float* norm, const float* lnorm,
                             const double* inv_mw, int ns, const double* P, const double* T, int64_t ng,
-                            const double* Y, double* wdot, float* err_est, void* stream);
+                            const double* Y, double* wdot, float* err_est, const double* range, void* stream);
 int chemgen_surrogate_infer_error(int reset);
 
 /* FP64 getrates that allocates no device memory (no counterpart in the

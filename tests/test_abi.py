@@ -67,7 +67,7 @@ def test_surrogate_and_mlp_entry_points_validate_arguments_without_a_gpu():
     assert L.chemgen_surrogate_targets(p, 8, 53, 53, p, p, None) == 1                   # dout < ns + 1
     assert L.chemgen_surrogate_decode(p, 8, 53, 54, p, p, 0, None) == 1                # dout < ns + 2
     # fused inference
-    infer = lambda img, ns, ng: L.chemgen_surrogate_infer(img, p, p, p, p, ns, p, p, ng, p, p, 0, None)
+    infer = lambda img, ns, ng: L.chemgen_surrogate_infer(img, p, p, p, p, ns, p, p, ng, p, p, 0, 0, None)
     assert infer(None, 53, 8) == 1
     assert infer(p, 62, 8) == 6                                                         # ns beyond the outputs
     assert infer(p, 0, 8) == 6

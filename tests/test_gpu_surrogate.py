@@ -211,6 +211,34 @@ def test_fused_inference_matches_layer_by_layer(small_surrogate, ng):
     assert (e2 - e1).abs().max().item() < 0.05
 
 
+def test_fused_inference_flags_points_outside_training_support(small_surrogate):
+    """With the range check on, the fused kernel gives exactly the points that
+    in_range() rejects (T or P outside the training ranges, a negative Y_k, Y
+    not summing to 1, a NaN) an error estimate of +inf, as the layer-by-layer
+    path does, and leaves every other estimate as it was."""
+    import torch
+    sur = small_surrogate
+    ng = 1000
+    P, T, Y = sur.sample_states(ng, torch.Generator(device="cuda").manual_seed(7))
+    T[3] = sur.T_range[1] + 1.0
+    T[10] = sur.T_range[0] - 1.0
+    P[20] = sur.P_range[1] * 1.01
+    P[21] = sur.P_range[0] * 0.99
+    d = Y[5, 30] + 1e-3                 # negative Y_k, sum kept at 1
+    Y[5, 30] = -1e-3
+    Y[0, 30] += d
+    Y[2, 40] += 1e-3                    # sum 1.001
+    T[50] = float("nan")
+    bad = ~sur.in_range(P, T, Y)
+    assert bad.sum().item() == 7
+    _, e_plain = sur.predict(P, T, Y)
+    _, e_chk = sur.predict(P, T, Y, check_range=True)
+    _, e_lbl = sur.predict(P, T, Y, fused=False, check_range=True)
+    assert torch.isinf(e_chk[bad]).all() and torch.isinf(e_lbl[bad]).all()
+    assert torch.isfinite(e_chk[~bad]).all()
+    assert torch.equal(e_chk[~bad], e_plain[~bad])
+
+
 def test_fused_inference_rejects_bad_arguments(small_surrogate):
     import torch
     from chemgen_b200.runtime import lib
@@ -221,7 +249,7 @@ def test_fused_inference_rejects_bad_arguments(small_surrogate):
     args = [bias.data_ptr(), sur.norm.data_ptr(), sur.lnorm.data_ptr(), sur.inv_mw.data_ptr()]
     s = torch.cuda.current_stream().cuda_stream
     call = lambda im, ns, ng: lib().chemgen_surrogate_infer(im, *args, ns, P.data_ptr(), T.data_ptr(), ng,
-                                                            Y.data_ptr(), W.data_ptr(), 0, s)
+                                                            Y.data_ptr(), W.data_ptr(), 0, 0, s)
     assert call(0, sur.ns, 16) == 1
     assert call(img.data_ptr(), 62, 16) == 6       # more species than outputs
     assert call(img.data_ptr() + 2, sur.ns, 16) == 5

@@ -65,8 +65,11 @@ class _FakeSur:
         self.gm = _FakeGM()
         self.est = est
 
-    def predict(self, P, T, Y):
-        return -torch.stack([T * (k + 1) for k in range(Y.shape[0])]), self.est.clone()
+    def predict(self, P, T, Y, check_range=False):
+        est = self.est.clone()
+        if check_range:                 # as the real one: +inf outside the training support
+            est.masked_fill_(~self.in_range(P, T, Y), float("inf"))
+        return -torch.stack([T * (k + 1) for k in range(Y.shape[0])]), est
 
     def in_range(self, P, T, Y):
         return (T >= 300) & (T <= 2500)
