@@ -183,6 +183,38 @@ def run_reference(args, rank, world):
 
 
 # ------------------------------------------------------------------ our arm
+def link_step_seconds(Ph, Th, Yh, Wh, Pd, Td, Yd, Wd, reps: int = 5) -> float:
+    """Seconds for one step's host-link traffic alone: the inputs host to
+    device on one stream while wdot goes device to host on another (the
+    ceiling of the end-to-end leg, which overlaps the same copies with the
+    kernel)."""
+    import torch
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    cur = torch.cuda.current_stream()
+
+    def step():
+        s1.wait_stream(cur)
+        s2.wait_stream(cur)
+        with torch.cuda.stream(s1):
+            Pd.copy_(Ph, non_blocking=True)
+            Td.copy_(Th, non_blocking=True)
+            Yd.copy_(Yh, non_blocking=True)
+        with torch.cuda.stream(s2):
+            Wh.copy_(Wd, non_blocking=True)
+        cur.wait_stream(s1)
+        cur.wait_stream(s2)
+
+    times = []
+    for r in range(reps + 2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        step()
+        torch.cuda.synchronize()
+        if r >= 2:
+            times.append(time.perf_counter() - t0)
+    return sorted(times)[len(times) // 2]
+
+
 def max_over_ranks(x: float, world: int, device=None) -> float:
     """The maximum of a per-rank time over all ranks (every rank calls it)."""
     if world <= 1:
@@ -488,6 +520,7 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(k_e2e):
         gm_e2e.getrates_host(Ph, Th, Yh, out=Wh.numpy(), mode=mode_e2e)
     e2e_s = max_over_ranks((time.perf_counter() - t0) / max(k_e2e, 1), world, dev)
+    link_s = max_over_ranks(link_step_seconds(Ph, Th, Yh, Wh, Pd, Td, Yd, W), world, dev)
 
     if rank != 0:
         return
@@ -521,7 +554,12 @@ def run_ours(args, rank, world, local_rank):
             "cpu_baseline": cpu,
             "e2e": {"value": ng * world / e2e_s / 1e6, "unit": "Mpoints/s",
                     "h2d_bytes_per_step": (2 + mech.ns) * ng * 8, "d2h_bytes_per_step": mech.ns * ng * 8,
-                    "api": "chemgen_getrates_host (pinned host buffers, 3-stream chunked copies)"},
+                    "api": "chemgen_getrates_host (pinned host buffers, 3-stream chunked copies)",
+                    "link": {"ceiling": ng * world / link_s / 1e6, "unit": "Mpoints/s",
+                             "both_directions_gbs": (2 + 2 * mech.ns) * ng * 8 / link_s / 1e9,
+                             "frac": link_s / e2e_s,
+                             "how": "the step's inputs host->device and wdot device->host as plain pinned "
+                                    "copies on two streams at once, no kernel (median of 5)"}},
             "gpu_launches": args.steps,
             "clocks": clocks,
             "modes": {m: dict(results[m], err=err.get(m), roofline=roof(m)) for m in modes},
