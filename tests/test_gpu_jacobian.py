@@ -41,7 +41,13 @@ def _rel(a, b):
     return float((num / den).max())
 
 
-@pytest.mark.parametrize("factory", [synthetic.h2o2_10sp, synthetic.all_kinds, synthetic.gri_shape])
+def _wide_90():
+    """90 species, 150 reactions: a wider mechanism, whose per-point state
+    (4 x 90 doubles) and J (90 x 91) stress the scratch and J strides."""
+    return synthetic.synthetic_mechanism(90, 150, 12, 12, seed=11, name="synthetic_90_150")
+
+
+@pytest.mark.parametrize("factory", [synthetic.h2o2_10sp, synthetic.all_kinds, synthetic.gri_shape, _wide_90])
 def test_jacobian_matches_central_differences(factory):
     mech = factory()
     blob = pack.pack(mech).to_blob()
