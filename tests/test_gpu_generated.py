@@ -114,3 +114,30 @@ def test_fp64_only_module_leaves_mixed_on_the_table_kernels(tmp_path):
     e64 = oracle.errors(gm.getrates(Pd, Td, Yd, mode="fp64").cpu().numpy(), w_ref, S)
     emx = oracle.errors(gm.getrates(Pd, Td, Yd, mode="mixed").cpu().numpy(), w_ref, S)
     assert e64["norm_max"] <= 1e-10 and emx["norm_max"] <= 1e-6, (e64, emx)
+
+
+def test_tensor_memory_gibbs_terms_in_both_kernels(tmp_path):
+    """emit(tmem=True) keeps the Gibbs array in tensor memory in both kernels
+    (the default for the FP64 kernel when it lets the block grow; an option
+    for the mixed kernel, where it measured slower): both stay in parity with
+    the oracle on a ragged point count.  (A mechanism no other test loads:
+    kernel registration is process-wide.)"""
+    import ctypes
+    import torch
+    from chemgen_b200 import emit_cuda
+    from chemgen_b200.runtime import lib
+    mech = synthetic.synthetic_mechanism(20, 60, 4, 4, seed=91, name="synthetic_20_60_s91")
+    assert emit_cuda.emit(mech, tmem=True).count("cgg::tm_alloc") == 2
+    so = emit_cuda.build_module(mech, out=str(tmp_path / "tmem.so"), tmem=True)
+    lib()
+    ctypes.CDLL(so, mode=ctypes.RTLD_GLOBAL)
+    blob = pack.pack(mech).to_blob()
+    gm = GpuMechanism(blob)
+    assert gm.kernel_kind("fp64") == "generated" and gm.kernel_kind("mixed") == "generated"
+    P, T, Y = synthetic.states(mech.ns, 3017, seed=6)
+    S = oracle.rates(blob, P, T, Y, mech.nr)["S"]
+    w_ref = oracle.getrates(blob, P, T, Y)
+    Pd, Td, Yd = (torch.from_numpy(x).cuda() for x in (P, T, Y))
+    e64 = oracle.errors(gm.getrates(Pd, Td, Yd, mode="fp64").cpu().numpy(), w_ref, S)
+    emx = oracle.errors(gm.getrates(Pd, Td, Yd, mode="mixed").cpu().numpy(), w_ref, S)
+    assert e64["norm_max"] <= 1e-10 and emx["norm_max"] <= 1e-6, (e64, emx)
