@@ -23,6 +23,12 @@ _A_UNITS = {"MOLES": 1.0, "MOLECULES": 6.02214076e23}
 _KEYWORDS = {"ELEMENTS", "ELEM", "SPECIES", "SPEC", "THERMO", "REACTIONS", "REAC", "TRANSPORT", "END"}
 
 
+def _num(text: str) -> float:
+    """A Chemkin number (Fortran D exponents allowed); a negative zero reads as
+    +0.0, as ck2yaml writes it."""
+    return float(text.replace("D", "E").replace("d", "e")) + 0.0
+
+
 def _strip_comment(line: str) -> str:
     i = line.find("!")
     return (line if i < 0 else line[:i]).rstrip()
@@ -90,7 +96,7 @@ def parse_thermo(lines: List[str], wanted: Optional[List[str]] = None) -> Dict[s
             for j in range(5):
                 field = lk[15 * j: 15 * (j + 1)].strip()
                 if field:
-                    coefs.append(float(field.replace("D", "E").replace("d", "e")))
+                    coefs.append(_num(field))
         if len(coefs) < 14:
             raise ValueError(f"thermo record for {name} has {len(coefs)} coefficients")
         high, low = tuple(coefs[0:7]), tuple(coefs[7:14])
@@ -204,7 +210,7 @@ def mechanism_from_chemkin(text: str, therm_text: Optional[str] = None, name: st
         m = rate_re.match(line.strip())
         if m and ("=" in m.group(1)):
             raw.append({"eqn": m.group(1).replace(" ", ""),
-                        "arh": tuple(float(x.replace("D", "E").replace("d", "e")) for x in m.groups()[1:]),
+                        "arh": tuple(_num(x) for x in m.groups()[1:]),
                         "aux": []})
         else:
             if not raw:
@@ -229,7 +235,7 @@ def mechanism_from_chemkin(text: str, therm_text: Optional[str] = None, name: st
                 continue
             for key, vals in re.findall(r"([A-Za-z][^/\s]*)\s*/([^/]*)/", aux):
                 K = key.upper()
-                nums = [float(v.replace("D", "E").replace("d", "e")) for v in vals.split()]
+                nums = [_num(v) for v in vals.split()]
                 if K == "LOW":
                     low = (nums[0], nums[1], nums[2] * e_fac)
                 elif K == "TROE":

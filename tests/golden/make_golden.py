@@ -15,7 +15,7 @@ committed recipe that reads them).  For each mechanism it:
 4. saves ``<name>.npz``: the mechanism (JSON), P, T, Y[ns, ng], and wdot from
    the scalar and the vectorised generated code.
 
-Usage:  python tests/golden/make_golden.py [reference_root]
+Usage:  python tests/golden/make_golden.py <reference_root>   (or CHEMGEN_REFERENCE=<reference_root>)
 """
 from __future__ import annotations
 
@@ -139,7 +139,9 @@ def plog_mechanism() -> Mechanism:
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CHEMGEN_REFERENCE", "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CHEMGEN_REFERENCE", "")
+    if not ref or not os.path.isdir(os.path.join(ref, "ck_files")):
+        sys.exit("usage: make_golden.py <reference checkout> (or set CHEMGEN_REFERENCE)")
     ck = os.path.join(ref, "ck_files")
     jobs = [
         (load_mechanism(os.path.join(ck, "H2_burke/chem.yaml"), name="h2_burke", reference_compat=True), 504, 1),

@@ -45,6 +45,23 @@ def test_getrates_cuda_emits_compilable_source(tmp_path, src):
     assert r.returncode == 0, r.stderr[-2000:]
 
 
+def test_getrates_cuda_from_chemkin_input(tmp_path):
+    """--mech chem.inp --therm therm.dat: the Chemkin reader feeds the emitter."""
+    from test_chemkin import _inp_text, _species, _therm_text
+    (tmp_path / "chem.inp").write_text(_inp_text())
+    (tmp_path / "therm.dat").write_text(_therm_text(_species()))
+    out = tmp_path / "getrates.cu"
+    r = subprocess.run([sys.executable, os.path.join(REPO, "generate_chemistry.py"), "--mode", "getrates",
+                        "--language", "cuda", "--mech", str(tmp_path / "chem.inp"), "--therm",
+                        str(tmp_path / "therm.dat"), "--output", str(out)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    text = out.read_text()
+    assert "cg_gen_fp64" in text and "cg_gen_mixed" in text
+    from chemgen_b200.chemkin import mechanism_from_chemkin
+    m = mechanism_from_chemkin(_inp_text(), _therm_text(_species()))
+    assert (tmp_path / "getrates.blob").read_bytes() == pack.pack(m).to_blob()
+
+
 @pytest.mark.parametrize("precision,has64,has32,mask", [("fp64", True, False, 1), ("mixed", False, True, 2),
                                                          ("both", True, True, 3)])
 def test_precision_selects_the_generated_kernels(tmp_path, precision, has64, has32, mask):
