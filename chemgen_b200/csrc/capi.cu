@@ -5,6 +5,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -672,8 +674,32 @@ int chemgen_free_constants(void) {
     return CHEMGEN_OK;
 }
 
-void getrates_hip_wrapper_v1(double* P, double* Temp, int ng, double* Ysp, double* wdot, double* log_eg,
-                             double* log_c) {
+int chemgen_global_num_species(void) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_handle ? g_handle->ns : -1;
+}
+
+int chemgen_init_constants_file(const char* path) {
+    if (!path || !*path) path = getenv("CHEMGEN_BLOB");
+    if (!path || !*path) path = "getrates.blob";
+    FILE* f = fopen(path, "rb");
+    if (!f) return CHEMGEN_ERR_INVALID_ARGUMENT;
+    std::vector<unsigned char> buf;
+    unsigned char tmp[65536];
+    size_t n;
+    while ((n = fread(tmp, 1, sizeof tmp, f)) > 0) buf.insert(buf.end(), tmp, tmp + n);
+    const bool bad = ferror(f) != 0;
+    fclose(f);
+    if (bad || buf.empty()) return CHEMGEN_ERR_INVALID_ARGUMENT;
+    return chemgen_init_constants(buf.data(), buf.size());
+}
+
+}  // extern "C"
+
+namespace {
+// Body shared by the four wrapper symbols: FP64 getrates on the process-wide
+// mechanism, synchronous on the legacy default stream.
+void wrapper_body(double* P, double* Temp, int ng, double* Ysp, double* wdot, double* log_c) {
     std::lock_guard<std::mutex> lk(g_mu);
     chemgen_handle* h = g_handle;
     if (!h) {
@@ -700,10 +726,53 @@ void getrates_hip_wrapper_v1(double* P, double* Temp, int ng, double* Ysp, doubl
     } else {
         st = run_owned(h, CHEMGEN_MODE_FP64, P, Temp, ng, Ysp, wdot, 0);
     }
-    (void)log_eg;
     cudaError_t e = cudaDeviceSynchronize();    // synchronous, as hip_v1_cpp.j2:371
     if (st == CHEMGEN_OK && e != cudaSuccess) st = status_of(e);
     g_wrapper_status = st;
+}
+}  // namespace
+
+extern "C" {
+
+void getrates_hip_wrapper_v1(double* P, double* Temp, int ng, double* Ysp, double* wdot, double* log_eg,
+                             double* log_c) {
+    (void)log_eg;
+    wrapper_body(P, Temp, ng, Ysp, wdot, log_c);
+}
+
+void getrates_hip_wrapper_v2(double* P, double* Temp, int ng, double* Ysp, double* wdot, double* log_eg,
+                             double* log_c) {
+    (void)log_eg;
+    wrapper_body(P, Temp, ng, Ysp, wdot, log_c);
+}
+
+void getrates_hip_wrapper_v3(double* P, double* Temp, int ng, double* Ysp, double* wdot, double* log_eg,
+                             double* log_c) {
+    (void)log_eg;
+    wrapper_body(P, Temp, ng, Ysp, wdot, log_c);
+}
+
+void getrates_hip_wrapper_v4(double* P, double* Temp, int ng, double* Ysp, double* wdot, double* log_eg,
+                             double* log_c) {
+    (void)log_eg;
+    wrapper_body(P, Temp, ng, Ysp, wdot, log_c);
+}
+
+void allocate_intermediate_DeviceMemory(int ng) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    chemgen_handle* h = g_handle;
+    if (!h) {
+        g_wrapper_status = CHEMGEN_ERR_NO_GLOBAL_MECHANISM;
+        return;
+    }
+    if (ng < 0) {
+        g_wrapper_status = CHEMGEN_ERR_INVALID_ARGUMENT;
+        return;
+    }
+    DeviceGuard g(h->device);
+    std::lock_guard<std::mutex> hl(h->mu);
+    const size_t need = ws_bytes_for(h, CHEMGEN_MODE_FP64, ng);
+    g_wrapper_status = need ? ensure_ws_locked(h, need) : CHEMGEN_OK;
 }
 
 int chemgen_last_wrapper_status(void) { return g_wrapper_status; }

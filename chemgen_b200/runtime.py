@@ -56,8 +56,14 @@ def lib() -> ctypes.CDLL:
     L.chemgen_getrates_host.argtypes = [vp, ci, vp, vp, i64, vp, vp]
     L.chemgen_init_constants.argtypes = [vp, sz]
     L.chemgen_free_constants.argtypes = []
-    L.getrates_hip_wrapper_v1.argtypes = [vp, vp, ci, vp, vp, vp, vp]
-    L.getrates_hip_wrapper_v1.restype = None
+    for v in (1, 2, 3, 4):
+        f = getattr(L, f"getrates_hip_wrapper_v{v}")
+        f.argtypes = [vp, vp, ci, vp, vp, vp, vp]
+        f.restype = None
+    L.allocate_intermediate_DeviceMemory.argtypes = [ci]
+    L.allocate_intermediate_DeviceMemory.restype = None
+    L.chemgen_init_constants_file.argtypes = [ctypes.c_char_p]
+    L.chemgen_global_num_species.argtypes = []
     L.chemgen_last_wrapper_status.argtypes = []
     L.chemgen_probe_math.argtypes = [vp, ci, vp, vp, vp, vp]
     L.chemgen_probe_math.restype = ci
@@ -92,6 +98,7 @@ def lib() -> ctypes.CDLL:
     for f in ("chemgen_create", "chemgen_destroy", "chemgen_num_species", "chemgen_num_reactions",
               "chemgen_getrates", "chemgen_getrates_ex", "chemgen_workspace_bytes", "chemgen_getrates_ws",
               "chemgen_getrates_host", "chemgen_init_constants", "chemgen_free_constants",
+              "chemgen_init_constants_file", "chemgen_global_num_species",
               "chemgen_last_wrapper_status", "chemgen_use_generated", "chemgen_kernel_kind",
               "chemgen_register_kernels", "chemgen_jacobian", "chemgen_getrates_vjp"):
         getattr(L, f).restype = ci

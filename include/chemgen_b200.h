@@ -199,6 +199,41 @@ void getrates_hip_wrapper_v1(double* P, double* Temp, int ng, double* Ysp, doubl
                              double* log_c);
 int chemgen_last_wrapper_status(void);
 
+/* The reference's Fortran module chemgen_m picks one of four wrappers at
+ * build time (chemgen/templates/chemgen_mod.j2:139-166): v2, the fused
+ * shared-memory kernel (reactions_hip/hip_v2_cpp.j2:1078-1160), v3, the
+ * species-split reduction (hip_v3_cpp.j2:1144), and v4, the rocBLAS
+ * formulation (hip_v4_cpp.j2:422, declared in hip_v4_h.j2:26-32).  All four
+ * keep v1's signature and meaning, and here all four run the same kernels:
+ * whichever the solver was built against links. */
+void getrates_hip_wrapper_v2(double* P, double* Temp, int ng, double* Ysp, double* wdot, double* log_eg,
+                             double* log_c);
+void getrates_hip_wrapper_v3(double* P, double* Temp, int ng, double* Ysp, double* wdot, double* log_eg,
+                             double* log_c);
+void getrates_hip_wrapper_v4(double* P, double* Temp, int ng, double* Ysp, double* wdot, double* log_eg,
+                             double* log_c);
+
+/* Replaces allocate_intermediate_DeviceMemory (chemgen/constants.py:435-470),
+ * which chemgen_m::init_chemgen calls for v4: here it reserves the
+ * library-owned scratch that FP64 calls of up to ng points on the
+ * process-wide mechanism need (none when the state fits in shared memory), so
+ * that later wrapper calls do not allocate.  Returns void like the reference;
+ * chemgen_last_wrapper_status() reports the outcome. */
+void allocate_intermediate_DeviceMemory(int ng);
+
+/* chemgen_init_constants from a blob file (generate_chemistry.py writes it
+ * beside the kernels): path, or when path is NULL or empty the file named by
+ * the environment variable CHEMGEN_BLOB, else "getrates.blob" in the working
+ * directory.  For callers such as Fortran init_chemgen(flag, ng) whose
+ * signature names no mechanism (chemgen/templates/chemgen_mod.j2:108-137). */
+int chemgen_init_constants_file(const char* path);
+
+/* Species count of the process-wide mechanism (-1 before
+ * chemgen_init_constants): what chemgen_m sizes its EG and C scratch with,
+ * where the reference's generated module has it as a constant
+ * (chemgen/templates/chemgen_mod.j2:118-120). */
+int chemgen_global_num_species(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -77,3 +77,48 @@ def test_surrogate_and_mlp_entry_points_validate_arguments_without_a_gpu():
     assert L.chemgen_surrogate_pack(p, p, p, None, p, None) == 1
     assert L.chemgen_surrogate_pack(p, p, p, p, p + 8, None) == 5
     assert L.chemgen_surrogate_image_elems() == 256 * 128 + 2 * 256 * 256 + 64 * 256
+
+
+def _c_prototypes():
+    """name -> number of parameters, for every function include/chemgen_b200.h declares."""
+    text = open(os.path.join(REPO, "include", "chemgen_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for m in re.finditer(r"([a-zA-Z_][a-zA-Z0-9_]*)\s*\(([^()]*)\)\s*;", text):
+        args = m.group(2).strip()
+        out[m.group(1)] = 0 if args in ("", "void") else len(args.split(","))
+    return out
+
+
+def test_fortran_module_binds_exported_symbols_with_matching_arity():
+    """include/chemgen_m.F90 (no Fortran compiler in this image): every
+    bind(C) interface names a symbol the library exports and the header
+    declares, with the header's number of arguments; the public names are
+    the reference module's (chemgen/templates/chemgen_mod.j2:22-23)."""
+    text = open(os.path.join(REPO, "include", "chemgen_m.F90")).read()
+    protos = _c_prototypes()
+    L = runtime.lib()
+    binds = re.findall(r"(?:subroutine|function)\s+(\w+)\s*\(([^)]*)\)\s*bind\(C,\s*name=\"(\w+)\"\)", text)
+    assert len(binds) >= 9
+    for fname, args, cname in binds:
+        assert fname == cname
+        assert hasattr(L, cname), cname
+        nargs = 0 if not args.strip() else len(args.split(","))
+        assert protos.get(cname) == nargs, (cname, nargs, protos.get(cname))
+    assert {f"getrates_hip_wrapper_v{v}" for v in (1, 2, 3, 4)} <= {c for _, _, c in binds}
+    assert re.search(r"public\s*::\s*init_chemgen", text) and re.search(r"public\s*::\s*getrates_gpu", text)
+    assert re.search(r"subroutine init_chemgen\(flag, ng\)", text)
+    assert re.search(r"subroutine getrates_gpu\(P, T, ng, Y, wdot\)", text)
+
+
+def test_process_wide_entry_points_fail_cleanly_without_a_mechanism(tmp_path):
+    L = runtime.lib()
+    assert L.chemgen_global_num_species() == -1
+    L.allocate_intermediate_DeviceMemory(16)
+    assert L.chemgen_last_wrapper_status() == 8
+    assert L.chemgen_init_constants_file(str(tmp_path / "missing.blob").encode()) == 1
+    (tmp_path / "empty.blob").write_bytes(b"")
+    assert L.chemgen_init_constants_file(str(tmp_path / "empty.blob").encode()) == 1
+    for v in (1, 2, 3, 4):
+        getattr(L, f"getrates_hip_wrapper_v{v}")(0, 0, 1, 0, 0, 0, 0)
+        assert L.chemgen_last_wrapper_status() == 8

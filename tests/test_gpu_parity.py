@@ -154,6 +154,42 @@ def test_reference_wrapper_drop_in():
     assert lib().chemgen_last_wrapper_status() == 8
 
 
+@pytest.mark.parametrize("version", [1, 2, 3, 4])
+def test_fortran_module_call_sequence(tmp_path, monkeypatch, version):
+    """What chemgen_m (include/chemgen_m.F90) does, through the same symbols:
+    init_chemgen loads the blob file named by CHEMGEN_BLOB, sizes EG and C from
+    chemgen_global_num_species, reserves scratch for v4, and getrates_gpu calls
+    getrates_hip_wrapper_v<version> (chemgen_mod.j2:108-166)."""
+    import torch
+    from chemgen_b200.runtime import lib
+    L = lib()
+    for name in ("h2_burke", "jetsurf2"):
+        mech, d = load_golden(name)
+        blob = pack.pack(mech).to_blob()
+        path = tmp_path / f"{name}.blob"
+        path.write_bytes(blob)
+        monkeypatch.setenv("CHEMGEN_BLOB", str(path))
+        assert L.chemgen_init_constants_file(None) == 0
+        ns = L.chemgen_global_num_species()
+        assert ns == mech.ns
+        ng = d["T"].size
+        if version == 4:
+            L.allocate_intermediate_DeviceMemory(ng)
+            assert L.chemgen_last_wrapper_status() == 0
+        Pt, Tt, Yt = (torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (d["P"], d["T"], d["Y"]))
+        w = torch.zeros_like(Yt)
+        eg = torch.empty((ns, ng), dtype=torch.float64, device="cuda")
+        c = torch.empty((ns, ng), dtype=torch.float64, device="cuda")
+        getattr(L, f"getrates_hip_wrapper_v{version}")(Pt.data_ptr(), Tt.data_ptr(), ng, Yt.data_ptr(),
+                                                        w.data_ptr(), eg.data_ptr(), c.data_ptr())
+        assert L.chemgen_last_wrapper_status() == 0
+        S = oracle.rates(blob, d["P"], d["T"], d["Y"], mech.nr)["S"]
+        e = oracle.errors(w.cpu().numpy(), d["wdot_scalar"], S)
+        assert e["norm_max"] <= TOL_FP64, (name, e)
+    assert L.chemgen_free_constants() == 0
+    assert L.chemgen_global_num_species() == -1
+
+
 def test_bad_arguments_return_status():
     import torch
     from chemgen_b200.runtime import ChemgenError
