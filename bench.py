@@ -231,6 +231,22 @@ def whole_job_mpts(points_per_rank: int, world: int, ms_max: float) -> float:
     return points_per_rank * world / (ms_max * 1e-3) / 1e6
 
 
+def choose_head(modes, results, err, head_arg: str, world: int, device=None) -> str:
+    """The headline mode: the fastest whose error against the oracle (checked
+    on rank 0) is within 1e-6 normwise, or `head_arg` when it names a mode.
+    Under several ranks rank 0's choice is broadcast, so that every rank times
+    the same kernel whatever its own timings say."""
+    ok = [m for m in modes if m in err and err[m]["norm_max"] <= 1e-6] or modes[:1]
+    head = max(ok, key=lambda m: results[m]["value"]) if head_arg == "auto" or head_arg not in modes else head_arg
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        hv = torch.tensor([modes.index(head)], dtype=torch.int64, device=device)
+        dist.broadcast(hv, src=0)
+        head = modes[int(hv.item())]
+    return head
+
+
 def rank_states(ns: int, ng: int, rank: int):
     """The points rank `rank` evaluates: its own seeded draw (weak scaling)."""
     from chemgen_b200 import synthetic
@@ -489,13 +505,7 @@ def run_ours(args, rank, world, local_rank):
             err[m] = oracle.errors(w, w_ref, S)
         del t_rates
 
-    ok = [m for m in modes if m in err and err[m]["norm_max"] <= 1e-6] or modes[:1]
-    head = max(ok, key=lambda m: results[m]["value"]) if args.head == "auto" or args.head not in modes else args.head
-    if world > 1:
-        # every rank runs the mode rank 0 chose
-        hv = torch.tensor([modes.index(head)], dtype=torch.int64, device=dev)
-        dist.broadcast(hv, src=0)
-        head = modes[int(hv.item())]
+    head = choose_head(modes, results, err, args.head, world, dev)
 
     # clocks during a timed pass of the headline mode
     sampler = ClockSampler(local_rank)

@@ -5,8 +5,12 @@
 //   ln2 split into a 32-bit head (k * head is exact for |k| < 2^20) and a
 //   tail; e^r from its Taylor series to degree 12 (truncation error
 //   < |r|^13/13! < 2e-16 relative); 2^k applied through the exponent field.
-//   Valid for |x| < 708 (cg_exp_clamped clamps first: results below 2^-1022
-//   flush to zero, above 2^1024 become +inf).
+//   Valid for |x| < 708.  cg_exp_clamped clamps x to [-746, 710] first.  At
+//   the ends 2^k is built from a biased exponent clamped to [0, 2047], so
+//   x <= -1022.5 ln2 (about -708.75, results below 2^-1022.5) flushes to zero,
+//   and x >= 1023.5 ln2 (about 709.44, results above 2^1023.5 = 1.3e308)
+//   gives +inf although e^x stays finite up to x = 709.78: the kernels treat
+//   rates that large as an overflow.
 // cg_log(x): x = 2^e m with m in [sqrt(1/2), sqrt(2)); ln m = 2 atanh(s),
 //   s = (m-1)/(m+1), |s| <= 0.1716, from the odd series of atanh to s^21
 //   (truncation < 3e-17); ln x = e ln2 + ln m.  Non-positive, infinite and

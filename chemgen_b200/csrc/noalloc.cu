@@ -9,15 +9,20 @@
 // of a library allocation.
 //
 // Limits and behaviour:
-// * the array holds kNoallocScratchBytes (16 MiB) on every GPU that loads the
-//   library, until the process exits;
+// * the array holds kNoallocScratchBytes (16 MiB) on every GPU where the
+//   module of this file has been loaded, until the process exits.  Under
+//   CUDA's lazy module loading (the default) that happens at the first use of
+//   the module on a device -- at the latest at this entry point's first call
+//   there, which may then allocate the array and synchronise the device.  A
+//   caller that must not allocate or synchronise in its loop makes one call
+//   per device during set-up;
 // * the kernel keeps 3*ns*64 doubles of state per resident block; a
 //   mechanism whose single block slice exceeds the array (ns > 10922) is
 //   rejected with CHEMGEN_ERR_TOO_LARGE; fewer slices than the GPU could run
 //   only lower the number of persistent blocks;
-// * the first call on a device looks up the array's device address
+// * the first call on a device also looks up the array's device address
 //   (cudaGetSymbolAddress) with that device current; make that first call
-//   before any stream capture;
+//   during set-up, before any stream capture;
 // * every call shares the one array: calls that overlap on the GPU (two
 //   streams, two host threads) race on it.  Each call writes every state
 //   value before reading it, so nothing has to start at zero.

@@ -174,13 +174,17 @@ int chemgen_surrogate_infer_error(int reset);
  * solver that owns the device memory pool or forbids allocation (and the
  * device synchronisation cudaMalloc/cudaFree can cause) inside its time-step
  * loop.  The per-point state that the large-mechanism FP64 kernel keeps in
- * scratch lives in a fixed 16 MiB device array inside the library (held on
- * every GPU that loads it until exit) instead of a library allocation.
- * Device pointers and layouts as chemgen_getrates.  A mechanism whose state
- * slice of 3*ns*64 doubles exceeds the array (ns > 10922) returns
- * CHEMGEN_ERR_TOO_LARGE.  The first call on a device looks up the array's
- * address (with that device current): make it before any stream capture.
- * All calls share the array, so calls that overlap on the GPU race. */
+ * scratch lives in a fixed 16 MiB device array inside the library instead of
+ * a library allocation; a GPU holds it from the moment the array's module is
+ * loaded there until exit.  Under CUDA's lazy module loading (the default)
+ * that load can happen at this entry point's first call on a device, and then
+ * allocates and may synchronise the device; that first call also looks up the
+ * array's address (with that device current).  So make one call per device
+ * during set-up, before any stream capture and outside any loop that must not
+ * allocate.  Device pointers and layouts as chemgen_getrates.  A mechanism
+ * whose state slice of 3*ns*64 doubles exceeds the array (ns > 10922) returns
+ * CHEMGEN_ERR_TOO_LARGE.  All calls share the array, so calls that overlap on
+ * the GPU race. */
 int chemgen_getrates_noalloc(chemgen_handle* h, const double* P, const double* T, int64_t ng, const double* Y,
                              double* wdot, void* stream);
 

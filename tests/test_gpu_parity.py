@@ -214,6 +214,16 @@ def test_kernel_exp_log_against_cuda_libm():
     ok = (er > 1e-300) & np.isfinite(er)
     assert np.max(np.abs(e[ok] - er[ok]) / er[ok]) < 1e-15
     assert np.all(np.isinf(e[np.isinf(er)]))
+    # the documented ends of cg_exp: +inf from x >= 1023.5 ln 2, zero at and
+    # below -1022.5 ln 2 (flushed, where CUDA's exp is subnormal)
+    hi = np.linspace(1023.5 * np.log(2) + 1e-12, 709.78, 64)
+    lo = np.linspace(-745.0, -1022.5 * np.log(2) - 1e-12, 64)
+    xe = torch.from_numpy(np.concatenate([hi, lo])).cuda()
+    oe = [torch.empty_like(xe) for _ in range(4)]
+    assert lib().chemgen_probe_math(ctypes_ptr(xe), xe.numel(), *(ctypes_ptr(o) for o in oe)) == 0
+    ee, _, eer, _ = (o.cpu().numpy() for o in oe)
+    assert np.all(np.isinf(ee[:64])) and np.all(np.isfinite(eer[:64]))
+    assert np.all(ee[64:] == 0.0) and np.all(eer[64:] < 2.0 ** -1022)
     ok = np.abs(lr) > 1e-3
     assert np.max(np.abs(l[ok] - lr[ok]) / np.abs(lr[ok])) < 1e-15
     assert np.max(np.abs(l - lr)) < 1e-15 * 800
