@@ -21,6 +21,11 @@ cudaError_t launch_getrates_fp64(const DevMech& m, const double* P, const double
 int fp64_smem_block(int ns, size_t smem_per_sm, size_t smem_per_block);
 size_t fp64_global_slice_bytes(int ns);
 int fp64_global_blocks_per_sm();
+struct StagedPlan;
+cudaError_t staged_prepare(const DevMech& m, const cg_mech_view& v, int device, StagedPlan** out);
+void staged_release(StagedPlan* p);
+cudaError_t launch_getrates_staged(const StagedPlan* p, const DevMech& m, const double* P, const double* T,
+                                   const double* Y, double* wdot, int64_t ng, cudaStream_t s);
 
 struct MixedPlan;
 cudaError_t mixed_prepare(const DevMech& m, const cg_mech_view& v, int device, MixedPlan** out);
@@ -49,7 +54,8 @@ struct chemgen_handle {
     cg::DevMech m{};
     void* dbuf = nullptr;
     int sm_count = 0;
-    int fp64_block = 0;             // 32/64/128: shared-memory state; 0: global scratch
+    int fp64_block = 0;             // 32/64/128: shared-memory state; 0: staged kernel or global scratch
+    cg::StagedPlan* staged = nullptr;   // FP64 staged kernel (state on chip) when fp64_block is 0
     int64_t fp64_slices = 0;        // persistent blocks of the global variant
     std::mutex mu;
     void* ws = nullptr;             // library-owned scratch
@@ -337,7 +343,7 @@ int ensure_ws_locked(chemgen_handle* h, size_t bytes) {
 }
 
 size_t fp64_ws_bytes(const chemgen_handle* h, int64_t ng) {
-    if (h->fp64_block) return 0;
+    if (h->fp64_block || h->staged) return 0;
     int64_t chunks = (ng + 63) / 64;
     int64_t slices = std::min<int64_t>(chunks, h->fp64_slices);
     return (size_t)slices * cg::fp64_global_slice_bytes(h->ns);
@@ -369,6 +375,8 @@ int launch(chemgen_handle* h, int mode, const double* P, const double* T, int64_
         (h->gen_modes & (1u << mode)))
         return h->gen_fn(mode, P, T, ng, Y, w, s);
     if (mode == CHEMGEN_MODE_FP64) {
+        if (!h->fp64_block && h->staged)
+            return status_of(cg::launch_getrates_staged(h->staged, h->m, P, T, Y, w, ng, s));
         int64_t slices = 0;
         if (!h->fp64_block) {
             if (!ws || (reinterpret_cast<uintptr_t>(ws) & 255u)) return CHEMGEN_ERR_INVALID_ARGUMENT;
@@ -467,6 +475,16 @@ int chemgen_create(const void* blob, size_t nbytes, int device, chemgen_handle**
     h->sm_count = prop.multiProcessorCount;
     h->fp64_block = cg::fp64_smem_block(h->ns, prop.sharedMemPerMultiprocessor, prop.sharedMemPerBlockOptin);
     h->fp64_slices = (int64_t)h->sm_count * cg::fp64_global_blocks_per_sm();
+    if (!h->fp64_block) {
+        // state too large for one thread per point in shared memory: the
+        // staged kernel when its tile fits, else the global-scratch kernel
+        e = cg::staged_prepare(h->m, v, device, &h->staged);
+        if (e != cudaSuccess && e != cudaErrorNotSupported) {
+            cudaFree(h->dbuf);
+            delete h;
+            return status_of(e);
+        }
+    }
     h->mixed_err = cg::mixed_prepare(h->m, v, device, &h->mixed);
     if (h->mixed_err == cudaErrorNotSupported) h->mixed_err = cudaSuccess;
     *out = h;
@@ -478,6 +496,7 @@ int chemgen_destroy(chemgen_handle* h) {
     DeviceGuard g(h->device);
     cudaDeviceSynchronize();
     if (h->mixed) cg::mixed_release(h->mixed);
+    if (h->staged) cg::staged_release(h->staged);
     if (h->ws) cudaFree(h->ws);
     if (h->dbuf) cudaFree(h->dbuf);
     if (h->iobuf) cudaFree(h->iobuf);
@@ -715,7 +734,7 @@ void wrapper_body(double* P, double* Temp, int ng, double* Ysp, double* wdot, do
     // Large mechanisms keep per-point state in scratch: the caller's log_c
     // (ng*ns doubles) when it holds at least one block's slice, otherwise
     // library-owned scratch.
-    if (!h->fp64_block && log_c) {
+    if (!h->fp64_block && !h->staged && log_c) {
         uintptr_t a = reinterpret_cast<uintptr_t>(log_c);
         uintptr_t al = (a + 255) & ~(uintptr_t)255;
         size_t bytes = (size_t)ng * h->ns * sizeof(double);

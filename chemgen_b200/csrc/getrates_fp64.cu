@@ -23,6 +23,10 @@
 // 16-byte loads.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <utility>
+#include <vector>
+
 #include "cg_math.cuh"
 #include "rates_common.cuh"
 
@@ -48,6 +52,61 @@ __device__ __forceinline__ void scatter_compact(const DRxn& R, double rr, double
             const int s = slot_species(R.sp[3 + j]);
             W[s * B] = fma((double)slot_nu(R.sp[3 + j]), rr, W[s * B]);
         }
+}
+
+// kb and the net rate of progress mfac * (qf - qb) of one reaction with
+// forward rate kf (reactions/standard.j2:3-19).  mfac is the third-body
+// concentration for three-body reactions, 1 otherwise (third_body.j2:30-31).
+// C and EGp are read with stride B.
+template <int B>
+__device__ __forceinline__ double net_rate(const DevMech& m, const DRxn& R, double kf, double mfac, const double* C,
+                                          const double* E) {
+    if (R.flags & kFCompact) {
+        double qf = kf, qb = 0.0;
+        if (R.flags & CG_F_REVERSIBLE) {
+            double num = 1.0, den = 1.0, cp = 1.0;
+#pragma unroll
+            for (int j = 0; j < kMaxCompact; ++j)
+                if (j < R.nre) num *= ipow3(E[slot_species(R.sp[j]) * B], slot_nu(R.sp[j]));
+#pragma unroll
+            for (int j = 0; j < kMaxCompact; ++j)
+                if (j < R.npr) {
+                    const int s = slot_species(R.sp[3 + j]), nu = slot_nu(R.sp[3 + j]);
+                    den *= ipow3(E[s * B], nu);
+                    cp *= ipow3(C[s * B], nu);
+                }
+            qb = kf * num * rcp_nr(den) * cp;
+        }
+#pragma unroll
+        for (int j = 0; j < kMaxCompact; ++j)
+            if (j < R.nre) qf *= ipow3(C[slot_species(R.sp[j]) * B], slot_nu(R.sp[j]));
+        return mfac * (qf - qb);
+    }
+    const int g = R.gen;
+    const int r0 = __ldg(m.gen_rptr + g), r1 = __ldg(m.gen_rptr + g + 1);
+    const int p0 = __ldg(m.gen_pptr + g), p1 = __ldg(m.gen_pptr + g + 1);
+    double qf = kf, qb = 0.0;
+    for (int j = r0; j < r1; ++j) {
+        const int s = __ldg(m.gen_sp + j);
+        const double nu = __ldg(m.gen_nu + j);
+        qf *= (nu == 1.0) ? C[s * B] : pow(C[s * B], nu);
+    }
+    if (R.flags & CG_F_REVERSIBLE) {
+        double ratio = 1.0, cp = 1.0;
+        for (int j = r0; j < r1; ++j) {
+            const int s = __ldg(m.gen_sp + j);
+            const double nu = __ldg(m.gen_nu + j);
+            ratio *= (nu == 1.0) ? E[s * B] : pow(E[s * B], nu);
+        }
+        for (int j = p0; j < p1; ++j) {
+            const int s = __ldg(m.gen_sp + j);
+            const double nu = __ldg(m.gen_nu + j);
+            ratio /= (nu == 1.0) ? E[s * B] : pow(E[s * B], nu);
+            cp *= (nu == 1.0) ? C[s * B] : pow(C[s * B], nu);
+        }
+        qb = kf * ratio * cp;
+    }
+    return mfac * (qf - qb);
 }
 
 // kb, q and the scatter for one reaction with forward rate kf.  mfac
@@ -287,6 +346,275 @@ __global__ void __launch_bounds__(B) getrates_fp64_global(DevMech m, const doubl
         const int64_t i = c * B + tid;
         getrates_point<B>(m, i < ng, i, ng, P, T, Y, wdot, st);
     }
+}
+
+// ------------------------------------------------ staged large-mechanism kernel
+//
+// For mechanisms whose per-point state is too large for a block of points in
+// shared memory with one thread per point and per-thread wdot (JetSurf-size,
+// hundreds of species).  A persistent CTA owns a tile of 32 points -- one
+// point per lane, so every lane of a warp works on the same reaction and no
+// branch diverges -- and keeps the tile's C and EGp in shared memory.  The
+// reactions run in chunks of R:
+//   pass 1  warp w computes the net rates of progress of reactions w, w + W,
+//           ... of the chunk for the 32 points into a staging array q[R][32];
+//   pass 2  warp w owns species w, w + W, ..., whose FP64 wdot accumulators
+//           sit in its registers for the whole tile, and adds
+//           sum_r nu_kr q_r over the chunk from a per-chunk species -> reaction
+//           list (reactions/standard.j2:21-27).
+// Each species has one owner, so the sums need no atomics and wdot is
+// written once per point, and nothing is kept in global scratch: DRAM traffic
+// is the inputs and outputs.
+
+struct StagedPlan {
+    int W = 16;                 // warps per CTA
+    int kpw = 0;                // accumulator slots per warp (template instance)
+    int R = 0;                  // reactions per chunk
+    int nchunk = 0;
+    size_t smem = 0;
+    int grid = 0;
+    const int* ptr = nullptr;   // [nchunk][ns + 1] into the entries
+    const int* er = nullptr;    // reaction of each entry, within its chunk
+    const double* enu = nullptr;  // net stoichiometric coefficient of each entry
+    void* dbuf = nullptr;
+};
+
+constexpr int kStTile = 32;
+
+template <int W, int KPW>
+__global__ void __launch_bounds__(32 * W, 1)
+    getrates_fp64_staged(DevMech m, int R, int nchunk, const int* __restrict__ cptr, const int* __restrict__ cer,
+                         const double* __restrict__ cnu, const double* __restrict__ P, const double* __restrict__ Tg,
+                         const double* __restrict__ Y, double* __restrict__ wdot, int64_t ng) {
+    extern __shared__ double smem[];
+    const int ns = m.ns;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double* sC = smem;                       // [ns][32]
+    double* sE = sC + ns * kStTile;          // [ns][32]
+    double* sQ = sE + ns * kStTile;          // [R][32]
+    double* sRed = sQ + R * kStTile;         // [W][32]
+    const int64_t ntiles = (ng + kStTile - 1) / kStTile;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t i = tile * kStTile + lane;
+        const bool act = i < ng;
+        const double T = act ? Tg[i] : 1000.0;
+        const double Pp = act ? P[i] : kPatm;
+        // ytoc.j2:3-18; species k handled by warp k % W, sums met in shared memory
+        double part = 0.0;
+        for (int k = warp; k < ns; k += W) {
+            const double c = (act ? Y[(int64_t)k * ng + i] : 1.0) * __ldg(m.inv_mw + k);
+            sC[k * kStTile + lane] = c;
+            part += c;
+        }
+        sRed[warp * kStTile + lane] = part;
+        __syncthreads();
+        double csum = 0.0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) csum += sRed[w * kStTile + lane];
+        const double fac = Pp / (kR0 * csum * T);
+        part = 0.0;
+        for (int k = warp; k < ns; k += W) {
+            const double c = sC[k * kStTile + lane] * fac;
+            sC[k * kStTile + lane] = c;
+            part += c;
+        }
+        PointT pt;
+        pt.T = T;
+        pt.lnT = cgm::cg_log(T);
+        pt.invT = 1.0 / T;
+        // exp_g.j2:2-27 with pfac = Patm/(R0 T) folded in
+        const double pfac = kPatm / (kR0 * T);
+        for (int k = warp; k < ns; k += W)
+            sE[k * kStTile + lane] = cgm::cg_exp_clamped(species_smh(m.thermo, k, T, pt.lnT, pt.invT)) * pfac;
+        __syncthreads();                     // csum read by every warp before sRed is reused
+        sRed[warp * kStTile + lane] = part;
+        __syncthreads();
+        double ctot = 0.0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) ctot += sRed[w * kStTile + lane];
+        const double lnP = cgm::cg_log(Pp);
+        double acc[KPW];
+#pragma unroll
+        for (int j = 0; j < KPW; ++j) acc[j] = 0.0;
+        const double* C = sC + lane;
+        const double* E = sE + lane;
+        for (int c = 0; c < nchunk; ++c) {
+            // pass 1: net rates of progress of this warp's reactions of the chunk
+            for (int rl = warp; rl < R; rl += W) {
+                const int r = c * R + rl;
+                double q = 0.0;
+                if (r < m.nr) {
+                    const DRxn Rx = load_rxn(m.rxn + r);
+                    int kind = CG_STANDARD;
+                    while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
+                    if (kind == CG_STANDARD) {
+                        q = net_rate<kStTile>(m, Rx, arrhenius(Rx.lnA, Rx.b, Rx.theta, Rx.sgn, pt), 1.0, C, E);
+                    } else if (kind == CG_THIRD_BODY) {
+                        double M = ctot;
+                        for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
+                            M = fma(__ldg(m.eff_val + e), C[__ldg(m.eff_sp + e) * kStTile], M);
+                        q = net_rate<kStTile>(m, Rx, arrhenius(Rx.lnA, Rx.b, Rx.theta, Rx.sgn, pt), M, C, E);
+                    } else if (kind == CG_PLOG) {
+                        q = net_rate<kStTile>(m, Rx, plog_kf(m, Rx.aux, Pp, lnP, pt), 1.0, C, E);
+                    } else {
+                        const DFall f = load_fall(m.fall + Rx.aux);
+                        const double x2 = __ldg(&m.fall2[Rx.aux].T2);
+                        double M = ctot;
+                        for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
+                            M = fma(__ldg(m.eff_val + e), C[__ldg(m.eff_sp + e) * kStTile], M);
+                        q = net_rate<kStTile>(m, Rx, falloff_kf(kind, Rx.flags, Rx, f, x2, M, pt), 1.0, C, E);
+                    }
+                }
+                sQ[rl * kStTile + lane] = q;
+            }
+            __syncthreads();
+            // pass 2: this warp's species accumulate the chunk's contributions
+            const int* cp = cptr + (int64_t)c * (ns + 1);
+#pragma unroll
+            for (int j = 0; j < KPW; ++j) {
+                const int k = warp + j * W;
+                if (k < ns) {
+                    const int e1 = __ldg(cp + k + 1);
+                    for (int e = __ldg(cp + k); e < e1; ++e)
+                        acc[j] = fma(__ldg(cnu + e), sQ[__ldg(cer + e) * kStTile + lane], acc[j]);
+                }
+            }
+            __syncthreads();
+        }
+        if (act) {
+#pragma unroll
+            for (int j = 0; j < KPW; ++j) {
+                const int k = warp + j * W;
+                if (k < ns) wdot[(int64_t)k * ng + i] = acc[j];
+            }
+        }
+    }
+}
+
+template <int W, int KPW>
+static const void* staged_fn() {
+    return (const void*)getrates_fp64_staged<W, KPW>;
+}
+
+static const void* staged_kernel(int kpw) {
+    switch (kpw) {
+        case 8: return staged_fn<16, 8>();
+        case 16: return staged_fn<16, 16>();
+        case 24: return staged_fn<16, 24>();
+        case 32: return staged_fn<16, 32>();
+        default: return nullptr;
+    }
+}
+
+cudaError_t staged_prepare(const DevMech& m, const cg_mech_view& v, int device, StagedPlan** out) {
+    *out = nullptr;
+    const int ns = m.ns, nr = m.nr;
+    StagedPlan pl;
+    pl.W = 16;
+    const int need = (ns + pl.W - 1) / pl.W;
+    pl.kpw = need <= 8 ? 8 : need <= 16 ? 16 : need <= 24 ? 24 : need <= 32 ? 32 : 0;
+    if (!pl.kpw || nr == 0) return cudaErrorNotSupported;
+    cudaDeviceProp prop;
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return e;
+    const size_t limit = prop.sharedMemPerBlockOptin;
+    const size_t fixed = (size_t)2 * ns * kStTile * 8 + (size_t)pl.W * kStTile * 8;
+    if (fixed + (size_t)pl.W * kStTile * 8 > limit) return cudaErrorNotSupported;
+    int R = (int)((limit - fixed) / (kStTile * 8));
+    R = std::min(R, 256) / pl.W * pl.W;
+    R = std::min(R, (nr + pl.W - 1) / pl.W * pl.W);
+    if (R < pl.W) return cudaErrorNotSupported;
+    pl.R = R;
+    pl.nchunk = (nr + R - 1) / R;
+    pl.smem = fixed + (size_t)R * kStTile * 8;
+    // per-chunk species -> (reaction, net nu) lists, reactions in kernel order
+    const int32_t* rp = (const int32_t*)v.a[CG_RPTR];
+    const int32_t* pp = (const int32_t*)v.a[CG_PPTR];
+    const int32_t* rsp = (const int32_t*)v.a[CG_RSP];
+    const int32_t* psp = (const int32_t*)v.a[CG_PSP];
+    const double* rnu = (const double*)v.a[CG_RNU];
+    const double* pnu = (const double*)v.a[CG_PNU];
+    std::vector<int> ptr((size_t)pl.nchunk * (ns + 1), 0);
+    std::vector<int> er;
+    std::vector<double> enu;
+    std::vector<double> net(ns, 0.0);
+    std::vector<std::vector<std::pair<int, double>>> lists(ns);
+    for (int c = 0; c < pl.nchunk; ++c) {
+        for (auto& l : lists) l.clear();
+        for (int r = c * R; r < std::min(nr, (c + 1) * R); ++r) {
+            for (int j = rp[r]; j < rp[r + 1]; ++j) net[rsp[j]] -= rnu[j];
+            for (int j = pp[r]; j < pp[r + 1]; ++j) net[psp[j]] += pnu[j];
+            for (int j = rp[r]; j < rp[r + 1]; ++j)
+                if (net[rsp[j]] != 0.0) {
+                    lists[rsp[j]].push_back({r - c * R, net[rsp[j]]});
+                    net[rsp[j]] = 0.0;
+                }
+            for (int j = pp[r]; j < pp[r + 1]; ++j)
+                if (net[psp[j]] != 0.0) {
+                    lists[psp[j]].push_back({r - c * R, net[psp[j]]});
+                    net[psp[j]] = 0.0;
+                }
+            for (int j = rp[r]; j < rp[r + 1]; ++j) net[rsp[j]] = 0.0;
+        }
+        int* cp = ptr.data() + (size_t)c * (ns + 1);
+        cp[0] = (int)er.size();
+        for (int k = 0; k < ns; ++k) {
+            for (const auto& x : lists[k]) {
+                er.push_back(x.first);
+                enu.push_back(x.second);
+            }
+            cp[k + 1] = (int)er.size();
+        }
+    }
+    const size_t b_ptr = (ptr.size() * sizeof(int) + 255) / 256 * 256;
+    const size_t b_er = (std::max<size_t>(er.size(), 1) * sizeof(int) + 255) / 256 * 256;
+    const size_t b_nu = std::max<size_t>(enu.size(), 1) * sizeof(double);
+    StagedPlan* p = new StagedPlan(pl);
+    e = cudaMalloc(&p->dbuf, b_ptr + b_er + b_nu);
+    char* d = (char*)p->dbuf;
+    if (e == cudaSuccess) e = cudaMemcpy(d, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !er.empty()) e = cudaMemcpy(d + b_ptr, er.data(), er.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !enu.empty())
+        e = cudaMemcpy(d + b_ptr + b_er, enu.data(), enu.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(staged_kernel(p->kpw), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem);
+    if (e != cudaSuccess) {
+        if (p->dbuf) cudaFree(p->dbuf);
+        delete p;
+        return e;
+    }
+    p->ptr = (const int*)d;
+    p->er = (const int*)(d + b_ptr);
+    p->enu = (const double*)(d + b_ptr + b_er);
+    p->grid = prop.multiProcessorCount;
+    *out = p;
+    return cudaSuccess;
+}
+
+void staged_release(StagedPlan* p) {
+    if (!p) return;
+    if (p->dbuf) cudaFree(p->dbuf);
+    delete p;
+}
+
+cudaError_t launch_getrates_staged(const StagedPlan* p, const DevMech& m, const double* P, const double* T,
+                                   const double* Y, double* wdot, int64_t ng, cudaStream_t s) {
+    if (ng <= 0) return cudaSuccess;
+    const int64_t tiles = (ng + kStTile - 1) / kStTile;
+    const unsigned grid = (unsigned)std::min<int64_t>(tiles, p->grid);
+    const unsigned threads = 32u * (unsigned)p->W;
+#define CG_STAGED_LAUNCH(K)                                                                                  \
+    getrates_fp64_staged<16, K><<<grid, threads, p->smem, s>>>(m, p->R, p->nchunk, p->ptr, p->er, p->enu, P, T, \
+                                                               Y, wdot, ng)
+    switch (p->kpw) {
+        case 8: CG_STAGED_LAUNCH(8); break;
+        case 16: CG_STAGED_LAUNCH(16); break;
+        case 24: CG_STAGED_LAUNCH(24); break;
+        case 32: CG_STAGED_LAUNCH(32); break;
+        default: return cudaErrorInvalidValue;
+    }
+#undef CG_STAGED_LAUNCH
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- launchers

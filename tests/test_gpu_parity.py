@@ -112,20 +112,52 @@ def test_host_pointer_path_matches_device_path():
 
 
 def test_workspace_variant_large_mechanism():
+    """348 species: the FP64 staged kernel keeps its state on chip (no
+    workspace); the mixed tensor-core kernel keeps its Gibbs terms in the
+    caller's workspace."""
     mech, d = load_golden("jetsurf2")
     blob = pack.pack(mech).to_blob()
     gm = GpuMechanism(blob)
     import torch
     ng = d["T"].size
-    assert gm.workspace_bytes(ng) > 0        # 348 species: state in scratch
-    ws = torch.empty(gm.workspace_bytes(ng) // 8 + 64, dtype=torch.float64, device="cuda")
-    Pt, Tt, Yt = (torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (d["P"], d["T"], d["Y"]))
-    out = torch.empty_like(Yt)
-    gm.getrates_ws(Pt, Tt, Yt, out, ws)
-    torch.cuda.synchronize()
+    assert gm.workspace_bytes(ng, "fp64") == 0
+    assert gm.workspace_bytes(ng, "mixed") > 0
     S = oracle.rates(blob, d["P"], d["T"], d["Y"], mech.nr)["S"]
-    e = oracle.errors(out.cpu().numpy(), d["wdot_scalar"], S)
+    Pt, Tt, Yt = (torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (d["P"], d["T"], d["Y"]))
+    for mode, tol in (("fp64", TOL_FP64), ("mixed", 1e-6)):
+        wb = gm.workspace_bytes(ng, mode)
+        ws = torch.empty(wb // 8 + 64, dtype=torch.float64, device="cuda") if wb else None
+        out = torch.empty_like(Yt)
+        gm.getrates_ws(Pt, Tt, Yt, out, ws, mode=mode)
+        torch.cuda.synchronize()
+        e = oracle.errors(out.cpu().numpy(), d["wdot_scalar"], S)
+        assert e["norm_max"] <= tol, (mode, e)
+
+
+@pytest.mark.parametrize("name,ng", [("jetsurf2", 1), ("jetsurf2", 33), ("jetsurf2", 1000),
+                                     ("synthetic_348_2163", 777)])
+def test_staged_fp64_kernel_large_mechanisms(name, ng):
+    """The staged FP64 kernel (32-point tiles, C and EGp in shared memory,
+    reactions in chunks, species-owned register accumulators) at ragged
+    sizes, against the oracle and against the global-scratch FP64 kernel that
+    the no-allocation entry point runs."""
+    import torch
+    from chemgen_b200.runtime import lib
+    mech, _ = load_golden(name)
+    blob = pack.pack(mech).to_blob()
+    gm = GpuMechanism(blob)
+    assert gm.workspace_bytes(ng, "fp64") == 0
+    P, T, Y = synthetic.states(mech.ns, ng, seed=ng)
+    w = _run(gm, P, T, Y)
+    r = oracle.rates(blob, P, T, Y, mech.nr)
+    e = oracle.errors(w, r["wdot"], r["S"])
     assert e["norm_max"] <= TOL_FP64 and e["gross_max"] <= TOL_FP64, e
+    Pt, Tt, Yt = (torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (P, T, Y))
+    w2 = torch.empty_like(Yt)
+    assert lib().chemgen_getrates_noalloc(gm.handle, Pt.data_ptr(), Tt.data_ptr(), ng, Yt.data_ptr(),
+                                          w2.data_ptr(), torch.cuda.current_stream().cuda_stream) == 0
+    torch.cuda.synchronize()
+    assert oracle.errors(w, w2.cpu().numpy())["norm_max"] <= TOL_FP64
 
 
 def test_reference_wrapper_drop_in():

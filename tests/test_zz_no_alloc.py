@@ -25,7 +25,7 @@ def _dev(x):
 def test_noalloc_matches_allocating_entry_point_twice(which):
     import torch
     if which == "jetsurf2":
-        mech, _ = load_golden("jetsurf2")      # 348 species: both entry points keep state in scratch
+        mech, _ = load_golden("jetsurf2")      # 348 species: the no-alloc entry point keeps state in scratch
     else:
         mech = synthetic.h2o2_10sp()           # small: the allocating entry point keeps it in shared memory
     gm = GpuMechanism(pack.pack(mech).to_blob())
