@@ -137,16 +137,31 @@ def measured_peaks():
         return HBM_FALLBACK_GBS, "fallback"
 
 
-def ncu_traffic(mode: str, ns: int, nr: int):
-    """DRAM bytes per point of the getrates kernel from the committed ncu summary."""
-    path = os.path.join(REPO, "profiles", "getrates_traffic.txt")
+def _profile_row(fname: str, mode: str, ns: int, nr: int):
+    """Numbers after `mode ns nr` on the matching row of a committed ncu summary table."""
+    path = os.path.join(REPO, "profiles", fname)
     if not os.path.exists(path):
         return None
     for line in open(path):
         p = line.split()
-        if len(p) == 4 and not line.startswith("#") and p[0] == mode and int(p[1]) == ns and int(p[2]) == nr:
-            return float(p[3])
+        if len(p) >= 4 and not line.startswith("#") and p[0] == mode and int(p[1]) == ns and int(p[2]) == nr:
+            return [float(x) for x in p[3:]]
     return None
+
+
+def ncu_traffic(mode: str, ns: int, nr: int):
+    """DRAM bytes per point of the getrates kernel from the committed ncu summary."""
+    row = _profile_row("getrates_traffic.txt", mode, ns, nr)
+    return None if row is None else row[0]
+
+
+def ncu_issue(mode: str, ns: int, nr: int):
+    """Warp instructions issued per point, and the FP64 / FMA (FP32) / XU (MUFU) pipes'
+    active fractions, of the generated kernel from the committed ncu summary."""
+    row = _profile_row("getrates_issue.txt", mode, ns, nr)
+    if row is None or len(row) < 4:
+        return None
+    return {"warp_inst_per_point": row[0], "pipe_fp64": row[1], "pipe_fma": row[2], "pipe_xu": row[3]}
 
 
 # ------------------------------------------------------------ reference arm
@@ -542,18 +557,51 @@ def run_ours(args, rank, world, local_rank):
     if world == 1 and not args.no_configs:
         del W, Pd, Td, Yd
         configs = other_configs(args, stream)
+    sm_count = torch.cuda.get_device_properties(local_rank).multi_processor_count
+
     def roof(m):
+        """The roofline of the kernel timed in mode m.  FP64 kernel: bound by
+        its FP64 pipe, work = the rate law's FP64 flop-equivalents.  Mixed
+        kernel: its exponents run in FP64, 2^f on the SFU and the products in
+        FP32, so no single pipe carries the work; what bounds it is the issue
+        rate (4 warp instructions per clock per SM), achieved = the warp
+        instructions it issues per point (ncu, committed) x points/s, peak at
+        the SM clock sampled while it ran.  Both report the other measure
+        beside it, and the HBM fraction."""
         ms = results[m]["ms_per_step"]
-        achieved = flop_pt * ng / (ms * 1e-3) / 1e12
-        return {"bound": "fp64", "achieved": achieved, "peak": fma_tf.value, "unit": "TFLOP/s",
-                "frac": achieved / fma_tf.value,
-                "traffic": (lambda b: None if b is None else b * ng)(ncu_traffic(m, mech.ns, mech.nr)),
+        fp64_achieved = flop_pt * ng / (ms * 1e-3) / 1e12
+        fp64 = {"achieved": fp64_achieved, "peak": fma_tf.value, "unit": "TFLOP/s",
+                "frac": fp64_achieved / fma_tf.value,
                 "peak_source": "FP64 FMA rate measured live on this GPU (chemgen_probe_fp64)",
                 "flop_equiv_per_point": flop_pt,
-                "transcendental_cost_fma": {"exp": c_exp.value, "log": c_log.value, "rcp": c_rcp.value},
-                "hbm": {"achieved_gbs": bytes_pt * ng / (ms * 1e-3) / 1e9, "peak_gbs": hbm_peak,
-                        "frac": bytes_pt * ng / (ms * 1e-3) / 1e9 / hbm_peak, "peak_source": hbm_src,
-                        "bytes_per_point": bytes_pt}}
+                "transcendental_cost_fma": {"exp": c_exp.value, "log": c_log.value, "rcp": c_rcp.value}}
+        traffic = ncu_traffic(m, mech.ns, mech.nr)
+        hbm = {"achieved_gbs": bytes_pt * ng / (ms * 1e-3) / 1e9, "peak_gbs": hbm_peak,
+               "frac": bytes_pt * ng / (ms * 1e-3) / 1e9 / hbm_peak, "peak_source": hbm_src,
+               "bytes_per_point": bytes_pt}
+        iss = ncu_issue(m, mech.ns, mech.nr) if results[m]["kernel"] == "generated" else None
+        issue = None
+        mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz")
+        if iss is not None and mhz:
+            a = iss["warp_inst_per_point"] * ng / (ms * 1e-3) / 1e9
+            pk = 4.0 * sm_count * mhz * 1e6 / 1e9
+            issue = {"achieved": a, "peak": pk, "unit": "Gwarp-inst/s", "frac": a / pk,
+                     "warp_inst_per_point": iss["warp_inst_per_point"],
+                     "peak_source": f"4 warp instructions per clock x {sm_count} SMs x {mhz:.0f} MHz "
+                                    "(SM clock sampled during the timed region)",
+                     "pipes_ncu": {k: iss[k] for k in ("pipe_fp64", "pipe_fma", "pipe_xu")}}
+        if m == "fp64" or issue is None:
+            out = {"bound": "fp64", **fp64, "traffic": None if traffic is None else traffic * ng}
+            if issue is not None:
+                out["issue"] = issue
+        else:
+            out = {"bound": "issue", **{k: issue[k] for k in ("achieved", "peak", "unit", "frac")},
+                   "traffic": None if traffic is None else traffic * ng,
+                   "peak_source": issue["peak_source"], "warp_inst_per_point": issue["warp_inst_per_point"],
+                   "pipes_ncu": issue["pipes_ncu"],
+                   "fp64_equivalent_frac": fp64["frac"], "fp64_equivalent": fp64}
+        out["hbm"] = hbm
+        return out
     line = {"metric": METRIC, "value": results[head]["value"], "unit": "Mpoints/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": results[head]["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

@@ -83,11 +83,16 @@ def lib() -> ctypes.CDLL:
     L.chemgen_surrogate_features.argtypes = [vp, vp, vp, i64, ci, ci, vp, vp, vp, vp, vp]
     L.chemgen_surrogate_targets.argtypes = [vp, i64, ci, ci, vp, vp, vp]
     L.chemgen_surrogate_decode.argtypes = [vp, i64, ci, ci, vp, vp, vp, vp]
+    L.chemgen_mlp_gemm_tc.argtypes = [vp, i64, vp, i64, ci, ci, ci, ci, vp, vp, i64, vp, i64, vp, i64, vp, i64,
+                                      ci, vp]
+    L.chemgen_mlp_tc_error.argtypes = [ci]
+    L.chemgen_mlp_transpose_bf16.argtypes = [vp, i64, ci, ci, vp, i64, vp]
     L.chemgen_surrogate_image_elems.argtypes = []
     L.chemgen_surrogate_pack.argtypes = [vp, vp, vp, vp, vp, vp]
     L.chemgen_surrogate_infer.argtypes = [vp, vp, vp, vp, vp, ci, vp, vp, i64, vp, vp, vp, vp, vp]
     L.chemgen_surrogate_infer_error.argtypes = [ci]
-    for f in ("chemgen_mlp_gemm", "chemgen_mlp_bias_gelu", "chemgen_mlp_gelu_backward", "chemgen_mlp_mse_grad",
+    for f in ("chemgen_mlp_gemm", "chemgen_mlp_gemm_tc", "chemgen_mlp_tc_error", "chemgen_mlp_transpose_bf16",
+              "chemgen_mlp_bias_gelu", "chemgen_mlp_gelu_backward", "chemgen_mlp_mse_grad",
               "chemgen_mlp_colsum", "chemgen_mlp_adam", "chemgen_surrogate_features", "chemgen_surrogate_targets",
               "chemgen_surrogate_decode", "chemgen_surrogate_image_elems", "chemgen_surrogate_pack",
               "chemgen_surrogate_infer", "chemgen_surrogate_infer_error"):

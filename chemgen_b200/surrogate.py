@@ -57,13 +57,43 @@ class TrainConfig:
     seed: int = 0
 
 
-class MLP:
-    """The network's parameters and the kernel calls of one forward/backward."""
+# epilogues of chemgen_mlp_gemm_tc
+EPI_STORE, EPI_STORE_T, EPI_BIAS_GELU, EPI_BIAS, EPI_GELU_BACK = 0, 1, 2, 3, 4
 
-    def __init__(self, din: int = DIN, hidden: int = HIDDEN, dout: int = DOUT, seed: int = 0, device: int = 0):
+
+def _p(t) -> int:
+    if t is None:
+        return 0
+    return t if isinstance(t, int) else t.data_ptr()
+
+
+def _gemm_tc(A, lda, B, ldb, M, N, K, epi, bias=None, zprev=None, ldz=0, C=None, ldc=0, H=None, ldh=0, HT=None,
+             ldt=0, accumulate=0):
+    check(lib().chemgen_mlp_gemm_tc(_p(A), lda, _p(B), ldb, M, N, K, epi, _p(bias), _p(zprev), ldz, _p(C), ldc, _p(H),
+                                    ldh, _p(HT), ldt, accumulate, _stream()), "mlp_gemm_tc")
+
+
+def _transpose(src, rows, cols, dst, lds=None, ldd=None):
+    check(lib().chemgen_mlp_transpose_bf16(_p(src), cols if lds is None else lds, rows, cols, _p(dst),
+                                           rows if ldd is None else ldd, _stream()), "mlp_transpose_bf16")
+
+
+class MLP:
+    """The network's parameters and the kernel calls of one forward/backward.
+
+    With `tc` (the default) the products run on the tensor cores through
+    chemgen_mlp_gemm_tc, each fused with its epilogue: bias + GELU in the
+    forward, GELU' in the input gradients; the weight gradients take the
+    transposed activations (written by the forward's epilogues) as K-major
+    operands.  A batch that is not a multiple of 128 rows, or tc=False, runs
+    on the warp-level chemgen_mlp_gemm with the separate elementwise kernels."""
+
+    def __init__(self, din: int = DIN, hidden: int = HIDDEN, dout: int = DOUT, seed: int = 0, device: int = 0,
+                 tc: bool = True):
         import torch
         g = torch.Generator(device="cpu").manual_seed(seed)
         self.dims = [din, hidden, hidden, hidden, dout]
+        self.tc = tc
         self.dev = torch.device("cuda", device)
         self.W: List = []       # FP32 master [N x K]
         self.Wb: List = []      # BF16 copy
@@ -78,6 +108,26 @@ class MLP:
         self.m = [torch.zeros_like(p) for p in self.params]
         self.v = [torch.zeros_like(p) for p in self.params]
         self._ws: Dict = {}
+        # operands of the tensor-core products: the first layer's weights twice
+        # side by side (its input is a hi + lo pair of BF16 parts), and the
+        # transposed weights [k x n] of the input-gradient products
+        self.Wd0 = torch.empty(hidden, 2 * din, dtype=torch.bfloat16, device=self.dev)
+        self.WT = [torch.empty(self.dims[l], self.dims[l + 1], dtype=torch.bfloat16, device=self.dev)
+                   for l in range(4)]
+        self.refresh_operands()
+
+    def refresh_operands(self):
+        """Rebuild Wd0 and the transposed weights from the BF16 weights (after
+        every optimizer step; part of the captured training step)."""
+        for l in range(4):
+            k, n = self.dims[l], self.dims[l + 1]
+            _transpose(self.Wb[l], n, k, self.WT[l])
+        din, hid = self.dims[0], self.dims[1]
+        _transpose(self.WT[0], din, hid, self.Wd0, ldd=2 * din)
+        _transpose(self.WT[0], din, hid, self.Wd0.data_ptr() + 2 * din, ldd=2 * din)
+
+    def _use_tc(self, B: int) -> bool:
+        return self.tc and B % 128 == 0
 
     def _buf(self, key, shape, dtype):
         import torch
@@ -97,12 +147,77 @@ class MLP:
             return [(X.data_ptr(), 2 * din), (X.data_ptr() + 2 * din, 2 * din)]
         raise ValueError(f"input width {X.shape[1]} is neither {din} nor {2 * din}")
 
+    def _forward_tc(self, X, keep: bool):
+        import torch
+        B = X.shape[0]
+        din, hid, dout = self.dims[0], self.dims[1], self.dims[4]
+        if X.shape[1] == 2 * din:
+            W0, K0 = self.Wd0, 2 * din
+        elif X.shape[1] == din:
+            W0, K0 = self.Wb[0], din
+        else:
+            raise ValueError(f"input width {X.shape[1]} is neither {din} nor {2 * din}")
+        self.acts, self.zs, self.actsT = [X], [], []
+        A, lda, Bw, K = X, X.shape[1], W0, K0
+        for l in range(3):
+            Z = self._buf(("Z", l, keep), (B, hid), torch.float32) if keep else None
+            H = self._buf(("H", l, keep), (B, hid), torch.bfloat16)
+            HT = self._buf(("HT", l), (hid, B), torch.bfloat16) if keep else None
+            _gemm_tc(A, lda, Bw, K, B, hid, K, EPI_BIAS_GELU, bias=self.b[l], C=Z, ldc=hid, H=H, ldh=hid, HT=HT,
+                     ldt=B)
+            self.zs.append(Z)
+            self.acts.append(H)
+            self.actsT.append(HT)
+            A, lda, Bw, K = H, hid, self.Wb[l + 1], hid
+        out = self._buf(("Z", 3, keep), (B, dout), torch.float32)
+        _gemm_tc(A, lda, Bw, K, B, dout, K, EPI_BIAS, bias=self.b[3], C=out, ldc=dout)
+        self.zs.append(out)
+        return out
+
+    def _backward_tc(self, dout_b, dout_f):
+        import torch
+        B = dout_b.shape[0]
+        s = _stream()
+        din, hid, dout = self.dims[0], self.dims[1], self.dims[4]
+        gW = [self._buf(("gW", l), (self.dims[l + 1], self.dims[l]), torch.float32) for l in range(4)]
+        gb = [self._buf(("gb", l), (self.dims[l + 1],), torch.float32) for l in range(4)]
+        doutT = self._buf(("doutT",), (dout, B), torch.bfloat16)
+        _transpose(dout_b, B, dout, doutT)
+        # layer 3: dW3[n][k] = sum_m dout[m][n] H2[m][k], as (H2^T)(dout^T)^T stored transposed
+        _gemm_tc(self.actsT[2], B, doutT, B, hid, dout, B, EPI_STORE_T, C=gW[3], ldc=hid)
+        check(lib().chemgen_mlp_colsum(dout_f.data_ptr(), gb[3].data_ptr(), B, dout, s), "mlp_colsum")
+        dZb, dZf, dZT, n = dout_b, dout_f, doutT, dout
+        for l in range(2, -1, -1):
+            # dZ_l = (dZ_{l+1} W_{l+1}) * GELU'(Z_l)
+            nb = self._buf(("dZb", l), (B, hid), torch.bfloat16)
+            nf = self._buf(("dZf", l), (B, hid), torch.float32)
+            nT = self._buf(("dZT", l), (hid, B), torch.bfloat16)
+            _gemm_tc(dZb, n, self.WT[l + 1], n, B, hid, n, EPI_GELU_BACK, zprev=self.zs[l], ldz=hid, C=nf, ldc=hid,
+                     H=nb, ldh=hid, HT=nT, ldt=B)
+            dZb, dZf, dZT, n = nb, nf, nT, hid
+            check(lib().chemgen_mlp_colsum(dZf.data_ptr(), gb[l].data_ptr(), B, hid, s), "mlp_colsum")
+            if l > 0:
+                # dW_l[n][k] = sum_m dZ_l[m][n] H_{l-1}[m][k]
+                _gemm_tc(dZT, B, self.actsT[l - 1], B, hid, hid, B, EPI_STORE, C=gW[l], ldc=hid)
+        # layer 0: the input's transposed parts (hi, lo) as operands, summed
+        X = self.acts[0]
+        w = X.shape[1]
+        XT = self._buf(("XT",), (w, B), torch.bfloat16)
+        _transpose(X, B, w, XT)
+        for j in range(w // din):
+            _gemm_tc(dZT, B, XT.data_ptr() + 2 * j * din * B, B, hid, din, B, EPI_STORE, C=gW[0], ldc=din,
+                     accumulate=1 if j else 0)
+        return gW + gb
+
     def forward(self, X, keep: bool = True):
         """X: BF16 [B, din], or [B, 2 din] holding hi and lo parts.  Returns
         the FP32 output [B, dout]; keeps Z_l and H_l for the backward when
         `keep`."""
         import torch
         B = X.shape[0]
+        self._tc_last = self._use_tc(B)
+        if self._tc_last:
+            return self._forward_tc(X, keep)
         s = _stream()
         H = X
         self.acts = [X]
@@ -128,6 +243,8 @@ class MLP:
         Returns the parameter gradients (same order as self.params)."""
         import torch
         B = dout_b.shape[0]
+        if getattr(self, "_tc_last", False):
+            return self._backward_tc(dout_b, dout_f)
         s = _stream()
         gW = [None] * 4
         gb = [None] * 4
@@ -165,6 +282,8 @@ class MLP:
             check(lib().chemgen_mlp_adam(p.data_ptr(), g.data_ptr(), self.m[j].data_ptr(), self.v[j].data_ptr(), wb,
                                          p.numel(), hyper.data_ptr(), b1, b2, eps, wd if j < 4 else 0.0, s),
                   "mlp_adam")
+        if self.tc:
+            self.refresh_operands()
 
 
 def adam_schedule(total: int, lr: float, lr_final: float, b1: float = 0.9, b2: float = 0.999, device=None):
@@ -399,6 +518,7 @@ class Surrogate:
                 check(lib().chemgen_mlp_adam(p.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(),
                                              0 if wb is None else wb.data_ptr(), p.numel(), hyper.data_ptr(), 0.9,
                                              0.999, 1e-8, 0.0, s), "mlp_adam")
+        self.net.refresh_operands()
         if log:
             log(f"error head: loss {loss.item() / max(steps, 1):.4e}")
 
@@ -420,6 +540,7 @@ class Surrogate:
             self.net.W[l].copy_(st["W"][l].to(self.dev))
             self.net.Wb[l].copy_(self.net.W[l].to(torch.bfloat16))
             self.net.b[l].copy_(st["b"][l].to(self.dev))
+        self.net.refresh_operands()
         self.norm.copy_(st["norm"].to(self.dev))
         self.lnorm.copy_(st["lnorm"].to(self.dev))
         self._img = None

@@ -162,6 +162,27 @@ int chemgen_surrogate_decode(const float* out, int64_t ng, int ns, int dout, con
  *   err_est = +inf, so that an error gate sends it to the exact kernel.  Asynchronous on `stream`.
  * chemgen_surrogate_infer_error: 1 if a bounded wait inside the kernel ever gave up (its outputs
  *   are then incomplete), 0 otherwise, -1 on a CUDA error; synchronous; reset != 0 clears it. */
+/* Training products on the tensor cores (tcgen05), each fused with what
+ * follows it (no counterpart in the reference).  chemgen_mlp_gemm_tc:
+ *   acc[m][n] = sum_k A[m*lda + k] B[n*ldb + k] (A [M x K], B [N x K], BF16,
+ *   K-major, 16-byte aligned, lda and ldb multiples of 8; M a multiple of 128,
+ *   N one of 32, 64 or a multiple of 128, K a multiple of 64), then epilogue
+ *   0 STORE          C[m*ldc + n] (+)= acc (accumulate != 0 adds)
+ *   1 STORE_T        C[n*ldc + m] (+)= acc
+ *   2 BIAS_GELU      z = acc + bias[n]; C = z (if C); H[m*ldh + n] and HT[n*ldt + m] = GELU(z) (BF16, if given)
+ *   3 BIAS           z = acc + bias[n]; C = z; H, HT = z (if given)
+ *   4 GELU_BACKWARD  d = acc * GELU'(zprev[m*ldz + n]); C = d (if C); H, HT = d (BF16, if given)
+ *   with GELU the tanh form of chemgen_mlp_bias_gelu.  Asynchronous on `stream`.
+ * chemgen_mlp_tc_error: 1 if a bounded wait inside chemgen_mlp_gemm_tc gave
+ *   up (outputs incomplete), else 0, -1 on a CUDA error; reset != 0 clears it.
+ * chemgen_mlp_transpose_bf16: dst[c*ldd + r] = src[r*lds + c], r < rows, c < cols. */
+int chemgen_mlp_gemm_tc(const void* A, int64_t lda, const void* B, int64_t ldb, int M, int N, int K, int epilogue,
+                        const float* bias, const float* zprev, int64_t ldz, float* C, int64_t ldc, void* H,
+                        int64_t ldh, void* HT, int64_t ldt, int accumulate, void* stream);
+int chemgen_mlp_tc_error(int reset);
+int chemgen_mlp_transpose_bf16(const void* src, int64_t lds, int rows, int cols, void* dst, int64_t ldd,
+                               void* stream);
+
 int chemgen_surrogate_image_elems(void);
 int chemgen_surrogate_pack(const void* W1, const void* W2, const void* W3, const void* W4, void* img, void* stream);
 int chemgen_surrogate_infer(const void* img, const float* bias, const float* norm, const float* lnorm,

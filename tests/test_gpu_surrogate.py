@@ -46,19 +46,112 @@ def test_mlp_gemm_all_stride_forms():
     assert lib().chemgen_mlp_gemm(A.data_ptr(), 45, 1, B.data_ptr(), 45, 1, C.data_ptr(), 10, 77, 33, 45, 0, s) == 1
 
 
+@pytest.mark.parametrize("M,N,K", [(128, 32, 64), (256, 64, 128), (256, 256, 256), (1024, 128, 1024),
+                                   (384, 256, 64)])
+def test_tcgen05_gemm_epilogues(M, N, K):
+    """chemgen_mlp_gemm_tc (tcgen05, BF16 in, FP32 accumulation in tensor
+    memory) against FP32 products of the same BF16 operands, for every
+    epilogue; GELU and GELU' against their tanh-form formulas."""
+    import torch
+    from chemgen_b200 import surrogate as S
+    from chemgen_b200.runtime import lib
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    A = (torch.randn(M, K, device="cuda", generator=g) / math.sqrt(K)).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    bias = torch.randn(N, device="cuda", generator=g)
+    zprev = torch.randn(M, N, device="cuda", generator=g)
+    ref = A.float() @ B.float().T
+    s = torch.cuda.current_stream().cuda_stream
+
+    def run(epi, C=None, ldc=0, H=None, HT=None, acc=0):
+        return lib().chemgen_mlp_gemm_tc(A.data_ptr(), K, B.data_ptr(), K, M, N, K, epi, bias.data_ptr(),
+                                         zprev.data_ptr(), N, 0 if C is None else C.data_ptr(), ldc,
+                                         0 if H is None else H.data_ptr(), N, 0 if HT is None else HT.data_ptr(), M,
+                                         acc, s)
+    C = torch.full((M, N), 3.0, device="cuda")
+    assert run(S.EPI_STORE, C, N) == 0
+    torch.cuda.synchronize()
+    assert torch.allclose(C, ref, rtol=1e-5, atol=1e-5)
+    assert run(S.EPI_STORE, C, N, acc=1) == 0
+    assert torch.allclose(C, 2 * ref, rtol=1e-5, atol=2e-5)
+    CT = torch.empty((N, M), device="cuda")
+    assert run(S.EPI_STORE_T, CT, M) == 0
+    assert torch.allclose(CT, ref.T, rtol=1e-5, atol=1e-5)
+    k0, k1 = 0.7978845608028654, 0.044715
+    z = ref + bias
+    t = torch.tanh(k0 * (z + k1 * z ** 3))
+    gelu = 0.5 * z * (1 + t)
+    H = torch.empty((M, N), dtype=torch.bfloat16, device="cuda")
+    HT = torch.empty((N, M), dtype=torch.bfloat16, device="cuda")
+    assert run(S.EPI_BIAS_GELU, C, N, H, HT) == 0
+    assert torch.allclose(C, z, rtol=1e-5, atol=1e-5)
+    assert torch.allclose(H.float(), gelu, rtol=2e-2, atol=2e-3)
+    assert torch.equal(HT, H.T.contiguous())
+    assert run(S.EPI_BIAS, C, N) == 0
+    assert torch.allclose(C, z, rtol=1e-5, atol=1e-5)
+    tp = torch.tanh(k0 * (zprev + k1 * zprev ** 3))
+    dg = 0.5 * (1 + tp) + 0.5 * zprev * (1 - tp * tp) * k0 * (1 + 3 * k1 * zprev ** 2)
+    assert run(S.EPI_GELU_BACK, C, N, H, HT) == 0
+    torch.cuda.synchronize()
+    assert torch.allclose(C, ref * dg, rtol=5e-3, atol=5e-3)
+    assert torch.equal(HT, H.T.contiguous()) and torch.equal(H, C.to(torch.bfloat16))
+    assert lib().chemgen_mlp_tc_error(1) == 0
+    # shapes the kernel does not tile are rejected before any launch
+    assert lib().chemgen_mlp_gemm_tc(A.data_ptr(), K, B.data_ptr(), K, M - 1, N, K, 0, 0, 0, 0, C.data_ptr(), N,
+                                     0, 0, 0, 0, 0, s) == 1
+    assert lib().chemgen_mlp_gemm_tc(A.data_ptr() + 2, K, B.data_ptr(), K, M, N, K, 0, 0, 0, 0, C.data_ptr(), N,
+                                     0, 0, 0, 0, 0, s) == 5
+
+
+def test_tensor_core_training_step_matches_warp_level_path():
+    """One forward + backward of the network through the tcgen05 products
+    (fused epilogues) against the warp-level products with the separate
+    elementwise kernels, same weights and batch."""
+    import torch
+    from chemgen_b200 import surrogate as S
+    from chemgen_b200.runtime import lib
+    B = 512
+    g = torch.Generator(device="cuda").manual_seed(5)
+    F = torch.randn(B, S.DIN, device="cuda", generator=g)
+    hi = F.to(torch.bfloat16)
+    X = torch.cat([hi, (F - hi.float()).to(torch.bfloat16)], dim=1).contiguous()
+    tgt = torch.randn(B, S.DOUT, device="cuda", generator=g)
+    colw = torch.ones(S.DOUT, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    res = {}
+    for tc in (True, False):
+        net = S.MLP(seed=4, tc=tc)
+        for bb in net.b:
+            bb.normal_(0.0, 0.1, generator=torch.Generator(device="cuda").manual_seed(9))
+        out = net.forward(X).clone()
+        db = torch.empty(B, S.DOUT, dtype=torch.bfloat16, device="cuda")
+        df = torch.empty(B, S.DOUT, device="cuda")
+        loss = torch.zeros(1, device="cuda")
+        assert lib().chemgen_mlp_mse_grad(out.data_ptr(), tgt.data_ptr(), colw.data_ptr(), db.data_ptr(),
+                                          df.data_ptr(), loss.data_ptr(), B, S.DOUT, s) == 0
+        res[tc] = (out, [x.clone() for x in net.backward(db, df)])
+    torch.cuda.synchronize()
+    assert lib().chemgen_mlp_tc_error(1) == 0
+    (o1, g1), (o0, g0) = res[True], res[False]
+    assert (o1 - o0).norm() / o0.norm() < 1e-3
+    for a, b in zip(g1, g0):
+        assert (a - b).norm() / b.norm() < 5e-3, ((a - b).norm() / b.norm()).item()
+
+
 # The kernels' GELU uses the hardware tanh approximation (relative error
 # about 2^-11); the oracle uses exact tanh.  With the BF16 roundings
 # restated, what is left is that approximation moving a fraction of the
 # activations across a BF16 rounding boundary: well under 5e-3 in norm.
+@pytest.mark.parametrize("tc", [True, False])
 @pytest.mark.parametrize("split", [False, True])
 @pytest.mark.parametrize("round_bf16,tol", [(True, 5e-3), (False, 5e-2)])
-def test_kernel_gradients_match_cpu_oracle(round_bf16, tol, split):
+def test_kernel_gradients_match_cpu_oracle(round_bf16, tol, split, tc):
     import torch
     from chemgen_b200 import surrogate as S
     from chemgen_b200.runtime import lib
     from oracle import mlp_ref
-    net = S.MLP(seed=3)
-    B = 192
+    net = S.MLP(seed=3, tc=tc)
+    B = 256 if tc else 192
     g = torch.Generator(device="cuda").manual_seed(1)
     F = torch.randn(B, S.DIN, device="cuda", generator=g)
     if split:
