@@ -35,6 +35,11 @@ cudaError_t launch_getrates_mixed(const MixedPlan* p, const DevMech& m, const do
                                   cudaStream_t s);
 size_t mixed_workspace_bytes(const MixedPlan* p, int64_t ng);
 size_t deriv_workspace_bytes(int ns, int64_t ng);
+struct JacPlan;
+cudaError_t jac_prepare(const DevMech& m, const cg_mech_view& v, int device, JacPlan** out);
+void jac_release(JacPlan* p);
+cudaError_t launch_jacobian_rows(const JacPlan* p, const DevMech& m, int precision, const double* P, const double* T,
+                                 const double* Y, void* J, int64_t ng, cudaStream_t s);
 cudaError_t launch_jacobian(const DevMech& m, int precision, const double* P, const double* T, const double* Y,
                             void* J, int64_t ng, double* scratch, int sm_count, cudaStream_t s);
 cudaError_t launch_vjp(const DevMech& m, const double* P, const double* T, const double* Y, const double* G, double* gT,
@@ -56,6 +61,7 @@ struct chemgen_handle {
     int sm_count = 0;
     int fp64_block = 0;             // 32/64/128: shared-memory state; 0: staged kernel or global scratch
     cg::StagedPlan* staged = nullptr;   // FP64 staged kernel (state on chip) when fp64_block is 0
+    cg::JacPlan* jac = nullptr;         // row-owner Jacobian (J written once) when its tile fits
     int64_t fp64_slices = 0;        // persistent blocks of the global variant
     std::mutex mu;
     void* ws = nullptr;             // library-owned scratch
@@ -485,6 +491,13 @@ int chemgen_create(const void* blob, size_t nbytes, int device, chemgen_handle**
             return status_of(e);
         }
     }
+    e = cg::jac_prepare(h->m, v, device, &h->jac);
+    if (e != cudaSuccess && e != cudaErrorNotSupported) {
+        if (h->staged) cg::staged_release(h->staged);
+        cudaFree(h->dbuf);
+        delete h;
+        return status_of(e);
+    }
     h->mixed_err = cg::mixed_prepare(h->m, v, device, &h->mixed);
     if (h->mixed_err == cudaErrorNotSupported) h->mixed_err = cudaSuccess;
     *out = h;
@@ -497,6 +510,7 @@ int chemgen_destroy(chemgen_handle* h) {
     cudaDeviceSynchronize();
     if (h->mixed) cg::mixed_release(h->mixed);
     if (h->staged) cg::staged_release(h->staged);
+    if (h->jac) cg::jac_release(h->jac);
     if (h->ws) cudaFree(h->ws);
     if (h->dbuf) cudaFree(h->dbuf);
     if (h->iobuf) cudaFree(h->iobuf);
@@ -525,6 +539,8 @@ int chemgen_jacobian(chemgen_handle* h, int precision, const double* P, const do
     if (precision != 0 && precision != 1) return CHEMGEN_ERR_INVALID_ARGUMENT;
     DeviceGuard g(h->device);
     if (h->max_side > 16) return CHEMGEN_ERR_UNSUPPORTED;
+    if (h->jac)
+        return status_of(cg::launch_jacobian_rows(h->jac, h->m, precision, P, T, Y, J, ng, (cudaStream_t)stream));
     std::lock_guard<std::mutex> lk(h->mu);
     st = ensure_ws_locked(h, cg::deriv_workspace_bytes(h->ns, ng));
     if (st) return st;

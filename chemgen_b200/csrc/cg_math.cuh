@@ -51,6 +51,11 @@ __device__ __forceinline__ double cg_exp(double x) {
 
 __device__ __forceinline__ double cg_exp_clamped(double x) { return cg_exp(fmin(fmax(x, -746.0), 710.0)); }
 
+// Out-of-line copies, for straight-line kernels whose code size (instruction
+// fetch) matters more than a call per use.
+static __device__ __noinline__ double cg_exp_ool(double x) { return cg_exp(x); }
+static __device__ __noinline__ double cg_exp_clamped_ool(double x) { return cg_exp_clamped(x); }
+
 __device__ __forceinline__ double cg_rcp(double x) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));

@@ -23,6 +23,10 @@
 // 4*ns*ng doubles laid out [array][species][point].
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <utility>
+#include <vector>
+
 #include "cg_math.cuh"
 #include "rates_common.cuh"
 
@@ -137,11 +141,27 @@ __device__ void plog_d(const DevMech& m, int row, double P, double lnP, const Po
 }
 
 // One side of a reaction: species, coefficients (compact or general rows).
-struct Side {
+// NMAX = 3 holds the compact form only; its loops unroll, so the arrays stay
+// in registers.
+template <int NMAX>
+struct SideT {
     int n;
-    int sp[16];
-    double nu[16];
+    int sp[NMAX];
+    double nu[NMAX];
 };
+using Side = SideT<16>;
+
+__device__ __forceinline__ void load_sides3(const DRxn& R, SideT<3>& re, SideT<3>& pr) {
+    re.n = R.nre;
+    pr.n = R.npr;
+#pragma unroll
+    for (int j = 0; j < kMaxCompact; ++j) {
+        re.sp[j] = slot_species(R.sp[j]);
+        re.nu[j] = slot_nu(R.sp[j]);
+        pr.sp[j] = slot_species(R.sp[3 + j]);
+        pr.nu[j] = slot_nu(R.sp[3 + j]);
+    }
+}
 
 __device__ __forceinline__ void load_sides(const DevMech& m, const DRxn& R, Side& re, Side& pr) {
     if (R.flags & kFCompact) {
@@ -186,11 +206,120 @@ __device__ __forceinline__ double dpowi(double x, double nu) {
 }
 
 // Derivative of prod_i c_i^nu_i with respect to factor j (product of the others).
-__device__ __forceinline__ double dprod(const Side& s, const double* c, int j) {
+template <int NMAX>
+__device__ __forceinline__ double dprod(const SideT<NMAX>& s, const double* c, int j) {
     double p = dpowi(c[j], s.nu[j]);
-    for (int i = 0; i < s.n; ++i)
-        if (i != j) p *= powi(c[i], s.nu[i]);
+#pragma unroll(NMAX == 3 ? 3 : 1)
+    for (int i = 0; i < NMAX; ++i)
+        if (i < s.n && i != j) p *= powi(c[i], s.nu[i]);
     return p;
+}
+
+// Rate of progress of reaction r at one point and its derivatives: dqdT at
+// fixed C, dqdM (three-body and falloff), and dq/dC_j over the reaction's own
+// species (dsp[0..nd)); re/pr are its sides.  State C, EGp and dE are read
+// with stride st.s.
+template <int NMAX>
+struct RxnGradT {
+    int kind;
+    bool usesM;
+    double qnet, dqdT, dqdM, dlkf_lnP;
+    int nd;
+    int dsp[2 * NMAX];
+    double dqc[2 * NMAX];
+};
+using RxnGrad = RxnGradT<16>;
+
+// NMAX = 3: compact reactions only (the caller checks kFCompact).
+template <int NMAX>
+__device__ __forceinline__ void reaction_grad(const DevMech& m, int r, const DRxn& R, const PointT& pt, double ctot,
+                                              double Pv, double lnP, const DState& st, SideT<NMAX>& re,
+                                              SideT<NMAX>& pr, RxnGradT<NMAX>& g) {
+    int kind = CG_STANDARD;
+    while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
+    if constexpr (NMAX == 3) load_sides3(R, re, pr);
+    else load_sides(m, R, re, pr);
+    double M = 0.0, kf, dlkf, gM = 0.0, dlkf_lnP = 0.0;
+    if (kind != CG_STANDARD && kind != CG_PLOG) {
+        M = ctot;
+        for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
+            M = fma(__ldg(m.eff_val + e), st.C[__ldg(m.eff_sp + e) * st.s], M);
+    }
+    if (kind == CG_STANDARD || kind == CG_THIRD_BODY) {
+        kf = R.sgn * cgm::cg_exp_clamped(arr_ln(R.lnA, R.b, R.theta, pt));
+        dlkf = arr_dln(R.b, R.theta, pt);
+    } else if (kind == CG_PLOG) {
+        plog_d(m, R.aux, Pv, lnP, pt, kf, dlkf, dlkf_lnP);
+    } else {
+        const DFall f = load_fall(m.fall + R.aux);
+        falloff_d(kind, R.flags, R, f, __ldg(&m.fall2[R.aux].T2), M, pt, kf, dlkf, gM);
+    }
+    double cr[NMAX], cp[NMAX];
+    double pf = 1.0;
+#pragma unroll(NMAX == 3 ? 3 : 1)
+    for (int j = 0; j < NMAX; ++j)
+        if (j < re.n) {
+            cr[j] = st.C[re.sp[j] * st.s];
+            pf *= powi(cr[j], re.nu[j]);
+        }
+    const double qf = kf * pf;
+    double kb = 0.0, qb = 0.0, dlKc = 0.0;
+    if (R.flags & CG_F_REVERSIBLE) {
+        double num = 1.0, den = 1.0, pb_ = 1.0;
+#pragma unroll(NMAX == 3 ? 3 : 1)
+        for (int j = 0; j < NMAX; ++j)
+            if (j < re.n) {
+                num *= powi(st.E[re.sp[j] * st.s], re.nu[j]);
+                dlKc = fma(re.nu[j], st.D[re.sp[j] * st.s], dlKc);
+            }
+#pragma unroll(NMAX == 3 ? 3 : 1)
+        for (int j = 0; j < NMAX; ++j)
+            if (j < pr.n) {
+                cp[j] = st.C[pr.sp[j] * st.s];
+                den *= powi(st.E[pr.sp[j] * st.s], pr.nu[j]);
+                pb_ *= powi(cp[j], pr.nu[j]);
+                dlKc = fma(-pr.nu[j], st.D[pr.sp[j] * st.s], dlKc);
+            }
+        kb = kf * num * cgm::cg_rcp(den);
+        qb = kb * pb_;
+    }
+    const double mfac = (kind == CG_THIRD_BODY) ? M : 1.0;
+    g.kind = kind;
+    g.qnet = qf - qb;
+    g.dlkf_lnP = dlkf_lnP;
+    g.dqdT = mfac * fma(qf, dlkf, -qb * (dlkf + dlKc));
+    g.dqdM = (kind == CG_THIRD_BODY) ? (qf - qb) : ((kind >= CG_LINDEMANN && kind <= CG_SRI) ? (qf - qb) * gM : 0.0);
+    g.usesM = kind >= CG_THIRD_BODY && kind <= CG_SRI;
+    const bool rev = (R.flags & CG_F_REVERSIBLE) != 0;
+    if constexpr (NMAX == 3) {
+        // fixed slots: 0..2 reactants, 3..5 products (unused: zero derivative
+        // on species 0), so that every loop over the slots unrolls
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const bool on = j < re.n;
+            g.dsp[j] = on ? re.sp[j] : 0;
+            g.dqc[j] = on ? mfac * kf * dprod(re, cr, j) : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const bool on = rev && j < pr.n;
+            g.dsp[3 + j] = on ? pr.sp[j] : 0;
+            g.dqc[3 + j] = on ? -mfac * kb * dprod(pr, cp, j) : 0.0;
+        }
+        g.nd = 6;
+    } else {
+        int nd = 0;
+        for (int j = 0; j < re.n; ++j) {
+            g.dsp[nd] = re.sp[j];
+            g.dqc[nd++] = mfac * kf * dprod(re, cr, j);
+        }
+        if (rev)
+            for (int j = 0; j < pr.n; ++j) {
+                g.dsp[nd] = pr.sp[j];
+                g.dqc[nd++] = -mfac * kb * dprod(pr, cp, j);
+            }
+        g.nd = nd;
+    }
 }
 
 template <bool JAC, typename JT>
@@ -243,66 +372,15 @@ __global__ void __launch_bounds__(128) deriv_kernel(DevMech m, const double* __r
         double tb = 0.0, ab = 0.0, pb = 0.0;
         const double lnP = cgm::cg_log(Pv);
         for (int r = 0; r < m.nr; ++r) {
-            const DRxn R = load_rxn(m.rxn + r);
-            int kind = CG_STANDARD;
-            while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
             Side re, pr;
-            load_sides(m, R, re, pr);
-            double M = 0.0, kf, dlkf, gM = 0.0, dlkf_lnP = 0.0;
-            if (kind != CG_STANDARD && kind != CG_PLOG) {
-                M = ctot;
-                for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
-                    M = fma(__ldg(m.eff_val + e), st.C[__ldg(m.eff_sp + e) * st.s], M);
-            }
-            if (kind == CG_STANDARD || kind == CG_THIRD_BODY) {
-                kf = R.sgn * cgm::cg_exp_clamped(arr_ln(R.lnA, R.b, R.theta, pt));
-                dlkf = arr_dln(R.b, R.theta, pt);
-            } else if (kind == CG_PLOG) {
-                plog_d(m, R.aux, Pv, lnP, pt, kf, dlkf, dlkf_lnP);
-            } else {
-                const DFall f = load_fall(m.fall + R.aux);
-                falloff_d(kind, R.flags, R, f, __ldg(&m.fall2[R.aux].T2), M, pt, kf, dlkf, gM);
-            }
-            double cr[16], cp[16];
-            double pf = 1.0;
-            for (int j = 0; j < re.n; ++j) {
-                cr[j] = st.C[re.sp[j] * st.s];
-                pf *= powi(cr[j], re.nu[j]);
-            }
-            const double qf = kf * pf;
-            double kb = 0.0, qb = 0.0, dlKc = 0.0;
-            if (R.flags & CG_F_REVERSIBLE) {
-                double num = 1.0, den = 1.0, pb_ = 1.0;
-                for (int j = 0; j < re.n; ++j) {
-                    num *= powi(st.E[re.sp[j] * st.s], re.nu[j]);
-                    dlKc = fma(re.nu[j], st.D[re.sp[j] * st.s], dlKc);
-                }
-                for (int j = 0; j < pr.n; ++j) {
-                    cp[j] = st.C[pr.sp[j] * st.s];
-                    den *= powi(st.E[pr.sp[j] * st.s], pr.nu[j]);
-                    pb_ *= powi(cp[j], pr.nu[j]);
-                    dlKc = fma(-pr.nu[j], st.D[pr.sp[j] * st.s], dlKc);
-                }
-                kb = kf * num * cgm::cg_rcp(den);
-                qb = kb * pb_;
-            }
-            const double mfac = (kind == CG_THIRD_BODY) ? M : 1.0;
-            const double dqdT = mfac * fma(qf, dlkf, -qb * (dlkf + dlKc));
-            const double dqdM = (kind == CG_THIRD_BODY) ? (qf - qb) : ((kind >= CG_LINDEMANN && kind <= CG_SRI) ? (qf - qb) * gM : 0.0);
-            const bool usesM = kind >= CG_THIRD_BODY && kind <= CG_SRI;
-            // dq/dC over the reaction's species (reactant slots then product slots)
-            double dqc[32];
-            int dsp[32];
-            int nd = 0;
-            for (int j = 0; j < re.n; ++j) {
-                dsp[nd] = re.sp[j];
-                dqc[nd++] = mfac * kf * dprod(re, cr, j);
-            }
-            if (R.flags & CG_F_REVERSIBLE)
-                for (int j = 0; j < pr.n; ++j) {
-                    dsp[nd] = pr.sp[j];
-                    dqc[nd++] = -mfac * kb * dprod(pr, cp, j);
-                }
+            RxnGrad rg;
+            const DRxn R = load_rxn(m.rxn + r);
+            reaction_grad<16>(m, r, R, pt, ctot, Pv, lnP, st, re, pr, rg);
+            const int kind = rg.kind, nd = rg.nd;
+            const double dqdT = rg.dqdT, dqdM = rg.dqdM;
+            const bool usesM = rg.usesM;
+            const int* dsp = rg.dsp;
+            const double* dqc = rg.dqc;
             if (JAC) {
                 JT* Jp = J + i;
                 // rows: every species of the reaction with its net coefficient contribution
@@ -335,7 +413,7 @@ __global__ void __launch_bounds__(128) deriv_kernel(DevMech m, const double* __r
                         gY[o] = fma(gq * dqdM, __ldg(m.eff_val + e), gY[o]);
                     }
                 }
-                if (kind == CG_PLOG) pb = fma(gq, (qf - qb) * dlkf_lnP / Pv, pb);
+                if (kind == CG_PLOG) pb = fma(gq, rg.qnet * rg.dlkf_lnP / Pv, pb);
             }
         }
         const double iS = 1.0 / S;
@@ -368,7 +446,232 @@ __global__ void __launch_bounds__(128) deriv_kernel(DevMech m, const double* __r
     }
 }
 
+// ------------------------------------------------ row-owner Jacobian kernel
+//
+// J written once.  A persistent CTA owns a tile of 32 points (one per lane,
+// so every lane of a warp evaluates the same reaction and nothing diverges)
+// and keeps the tile's C, EGp and dE in shared memory.  Warp w owns the rows
+// k = w, w + W, ...: for row k it walks the reactions that change species k
+// (a per-species list of (reaction, net nu), built once per mechanism),
+// evaluates each reaction's rate derivatives for its 32 points and adds
+// nu * dq into the row, held in a [ns + 1][32] shared-memory buffer of its
+// own; then it applies the chain rule through C(T, Y) (file header) and
+// stores the row's ns + 1 columns, one coalesced 32-point store each.  A
+// reaction is evaluated once per species it changes (about four times), in
+// exchange for J never being read back from memory.
+constexpr int kJTile = 32;
+constexpr int kJMaxWarps = 8;
+
+template <typename JT>
+__global__ void __launch_bounds__(32 * kJMaxWarps, 1)
+    jac_rows_kernel(DevMech m, const int* __restrict__ lptr, const int* __restrict__ lrx,
+                    const double* __restrict__ lnu, const double* __restrict__ P, const double* __restrict__ Tg,
+                    const double* __restrict__ Y, JT* __restrict__ J, int64_t ng) {
+    extern __shared__ double smem[];
+    const int ns = m.ns, ncol = ns + 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double* sC = smem;
+    double* sE = sC + ns * kJTile;
+    double* sD = sE + ns * kJTile;
+    double* sRed = sD + ns * kJTile;                               // [kJMaxWarps][32]
+    double* row = sRed + kJMaxWarps * kJTile + (size_t)warp * ncol * kJTile + lane;   // this warp's [ncol][32]
+    const int64_t ntiles = (ng + kJTile - 1) / kJTile;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t i = tile * kJTile + lane;
+        const bool act = i < ng;
+        const double T = act ? Tg[i] : 1000.0;
+        const double Pv = act ? P[i] : kPatm;
+        PointT pt;
+        pt.T = T;
+        pt.lnT = cgm::cg_log(T);
+        pt.invT = 1.0 / T;
+        double part = 0.0;
+        for (int k = warp; k < ns; k += nw) {
+            const double c = (act ? Y[(int64_t)k * ng + i] : 1.0) * __ldg(m.inv_mw + k);
+            sC[k * kJTile + lane] = c;
+            part += c;
+        }
+        sRed[warp * kJTile + lane] = part;
+        __syncthreads();
+        double S = 0.0;
+        for (int w = 0; w < nw; ++w) S += sRed[w * kJTile + lane];
+        const double fac = Pv / (kR0 * S * T);
+        const double pfac = kPatm / (kR0 * T);
+        part = 0.0;
+        for (int k = warp; k < ns; k += nw) {
+            const double c = sC[k * kJTile + lane] * fac;
+            sC[k * kJTile + lane] = c;
+            part += c;
+            const double* th = m.thermo + 16 * k;
+            const double* cf = (T < __ldg(th)) ? th + 1 : th + 8;
+            double cc[7];
+#pragma unroll
+            for (int j = 0; j < 7; ++j) cc[j] = __ldg(cf + j);
+            sE[k * kJTile + lane] = cgm::cg_exp_clamped(smh_poly(cc, T, pt.lnT, pt.invT)) * pfac;
+            const double dp = fma(fma(fma(4.0 * cc[5], T, 3.0 * cc[4]), T, 2.0 * cc[3]), T, cc[2]);
+            sD[k * kJTile + lane] = dp + fma(cc[6], pt.invT, cc[1]) * pt.invT - pt.invT;
+        }
+        __syncthreads();                     // S read by every warp before sRed is reused
+        sRed[warp * kJTile + lane] = part;
+        __syncthreads();
+        double ctot = 0.0;
+        for (int w = 0; w < nw; ++w) ctot += sRed[w * kJTile + lane];
+        const double lnP = cgm::cg_log(Pv);
+        const DState st{sC + lane, sE + lane, sD + lane, nullptr, kJTile};
+        const double iS = 1.0 / S;
+        for (int k = warp; k < ns; k += nw) {
+            for (int c = 0; c < ncol; ++c) row[c * kJTile] = 0.0;
+            double ak = 0.0;
+            const int e1 = __ldg(lptr + k + 1);
+            for (int e = __ldg(lptr + k); e < e1; ++e) {
+                const int r = __ldg(lrx + e);
+                const double nu = __ldg(lnu + e);
+                const DRxn R = load_rxn(m.rxn + r);
+                double dqdT, dqdM;
+                bool usesM;
+                if (R.flags & kFCompact) {
+                    SideT<3> re, pr;
+                    RxnGradT<3> g;
+                    reaction_grad<3>(m, r, R, pt, ctot, Pv, lnP, st, re, pr, g);
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) row[(1 + g.dsp[j]) * kJTile] = fma(nu, g.dqc[j], row[(1 + g.dsp[j]) * kJTile]);
+                    dqdT = g.dqdT;
+                    dqdM = g.dqdM;
+                    usesM = g.usesM;
+                } else {
+                    Side re, pr;
+                    RxnGrad g;
+                    reaction_grad<16>(m, r, R, pt, ctot, Pv, lnP, st, re, pr, g);
+                    for (int j = 0; j < g.nd; ++j)
+                        row[(1 + g.dsp[j]) * kJTile] = fma(nu, g.dqc[j], row[(1 + g.dsp[j]) * kJTile]);
+                    dqdT = g.dqdT;
+                    dqdM = g.dqdM;
+                    usesM = g.usesM;
+                }
+                row[0] = fma(nu, dqdT, row[0]);
+                if (usesM) {
+                    // dM/dC_j = 1 + (eff_j - 1): the 1 goes to every column (ak), the rest is sparse
+                    ak = fma(nu, dqdM, ak);
+                    for (int f = __ldg(m.eff_ptr + r); f < __ldg(m.eff_ptr + r + 1); ++f)
+                        row[(1 + __ldg(m.eff_sp + f)) * kJTile] =
+                            fma(nu * __ldg(m.eff_val + f), dqdM, row[(1 + __ldg(m.eff_sp + f)) * kJTile]);
+                }
+            }
+            // chain rule through C(T, Y): rk = sum_j dwdot_k/dC_j C_j
+            double rk = ak * ctot;
+            for (int j = 0; j < ns; ++j) rk = fma(row[(1 + j) * kJTile], sC[j * kJTile + lane], rk);
+            if (act) {
+                JT* Jr = J + (int64_t)k * ncol * ng + i;
+                Jr[0] = (JT)(row[0] - rk * pt.invT);
+                for (int j = 0; j < ns; ++j)
+                    Jr[(int64_t)(1 + j) * ng] = (JT)(fma(ctot, row[(1 + j) * kJTile] + ak, -rk) * __ldg(m.inv_mw + j) * iS);
+            }
+        }
+        __syncthreads();                     // the tile's state stays until every row is done
+    }
+}
+
 }  // namespace
+
+// Row-owner Jacobian plan: per-species (reaction, net nu) lists.
+struct JacPlan {
+    int warps = 0;
+    size_t smem = 0;
+    int grid = 0;
+    const int* lptr = nullptr;
+    const int* lrx = nullptr;
+    const double* lnu = nullptr;
+    void* dbuf = nullptr;
+};
+
+cudaError_t jac_prepare(const DevMech& m, const cg_mech_view& v, int device, JacPlan** out) {
+    *out = nullptr;
+    const int ns = m.ns, nr = m.nr;
+    cudaDeviceProp prop;
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return e;
+    const size_t fixed = (size_t)3 * ns * kJTile * 8 + (size_t)kJMaxWarps * kJTile * 8;
+    const size_t per_warp = (size_t)(ns + 1) * kJTile * 8;
+    if (fixed + 2 * per_warp > prop.sharedMemPerBlockOptin) return cudaErrorNotSupported;
+    const int warps = (int)std::min<size_t>(kJMaxWarps, (prop.sharedMemPerBlockOptin - fixed) / per_warp);
+    const int32_t* rp = (const int32_t*)v.a[CG_RPTR];
+    const int32_t* pp = (const int32_t*)v.a[CG_PPTR];
+    const int32_t* rsp = (const int32_t*)v.a[CG_RSP];
+    const int32_t* psp = (const int32_t*)v.a[CG_PSP];
+    const double* rnu = (const double*)v.a[CG_RNU];
+    const double* pnu = (const double*)v.a[CG_PNU];
+    std::vector<std::vector<std::pair<int, double>>> lists(ns);
+    std::vector<double> net(ns, 0.0);
+    for (int r = 0; r < nr; ++r) {
+        for (int j = rp[r]; j < rp[r + 1]; ++j) net[rsp[j]] -= rnu[j];
+        for (int j = pp[r]; j < pp[r + 1]; ++j) net[psp[j]] += pnu[j];
+        for (int j = rp[r]; j < rp[r + 1]; ++j)
+            if (net[rsp[j]] != 0.0) {
+                lists[rsp[j]].push_back({r, net[rsp[j]]});
+                net[rsp[j]] = 0.0;
+            }
+        for (int j = pp[r]; j < pp[r + 1]; ++j)
+            if (net[psp[j]] != 0.0) {
+                lists[psp[j]].push_back({r, net[psp[j]]});
+                net[psp[j]] = 0.0;
+            }
+    }
+    std::vector<int> lptr(ns + 1, 0), lrx;
+    std::vector<double> lnu;
+    for (int k = 0; k < ns; ++k) {
+        for (const auto& x : lists[k]) {
+            lrx.push_back(x.first);
+            lnu.push_back(x.second);
+        }
+        lptr[k + 1] = (int)lrx.size();
+    }
+    const size_t b_ptr = ((ns + 1) * sizeof(int) + 255) / 256 * 256;
+    const size_t b_rx = (std::max<size_t>(lrx.size(), 1) * sizeof(int) + 255) / 256 * 256;
+    const size_t b_nu = std::max<size_t>(lnu.size(), 1) * sizeof(double);
+    JacPlan* p = new JacPlan();
+    p->warps = warps;
+    p->smem = fixed + (size_t)warps * per_warp;
+    p->grid = prop.multiProcessorCount;
+    e = cudaMalloc(&p->dbuf, b_ptr + b_rx + b_nu);
+    char* d = (char*)p->dbuf;
+    if (e == cudaSuccess) e = cudaMemcpy(d, lptr.data(), lptr.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !lrx.empty()) e = cudaMemcpy(d + b_ptr, lrx.data(), lrx.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !lnu.empty())
+        e = cudaMemcpy(d + b_ptr + b_rx, lnu.data(), lnu.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(jac_rows_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(jac_rows_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem);
+    if (e != cudaSuccess) {
+        if (p->dbuf) cudaFree(p->dbuf);
+        delete p;
+        return e;
+    }
+    p->lptr = (const int*)d;
+    p->lrx = (const int*)(d + b_ptr);
+    p->lnu = (const double*)(d + b_ptr + b_rx);
+    *out = p;
+    return cudaSuccess;
+}
+
+void jac_release(JacPlan* p) {
+    if (!p) return;
+    if (p->dbuf) cudaFree(p->dbuf);
+    delete p;
+}
+
+cudaError_t launch_jacobian_rows(const JacPlan* p, const DevMech& m, int precision, const double* P, const double* T,
+                                 const double* Y, void* J, int64_t ng, cudaStream_t s) {
+    if (ng <= 0) return cudaSuccess;
+    const int64_t tiles = (ng + kJTile - 1) / kJTile;
+    const unsigned grid = (unsigned)std::min<int64_t>(tiles, p->grid);
+    const unsigned threads = 32u * (unsigned)p->warps;
+    if (precision == 0)
+        jac_rows_kernel<double><<<grid, threads, p->smem, s>>>(m, p->lptr, p->lrx, p->lnu, P, T, Y, (double*)J, ng);
+    else
+        jac_rows_kernel<float><<<grid, threads, p->smem, s>>>(m, p->lptr, p->lrx, p->lnu, P, T, Y, (float*)J, ng);
+    return cudaGetLastError();
+}
 
 size_t deriv_workspace_bytes(int ns, int64_t ng) { return (size_t)4 * ns * ng * sizeof(double); }
 

@@ -119,8 +119,10 @@ def _f(x: float) -> str:
 
 class _Emitter:
     def __init__(self, mech: Mechanism, block: int, sync_every: int = SYNC_EVERY, tmem: bool = False,
-                 live_order: bool = True):
+                 live_order: bool = True, exp_noinline: bool = False):
         self.sync_every = sync_every
+        # reactions call out-of-line copies of the FP64 exp (shorter code)
+        self.exp_noinline = exp_noinline
         # register accumulators: reactions in live-range order, each wdot
         # stored right after the last reaction that touches its species
         self.live_order = live_order and mech.ns <= MAX_REG_SPECIES
@@ -605,7 +607,11 @@ class _Emitter:
                 if new:
                     L.append("  double " + ", ".join(f"w{k} = 0.0" for k in new) + ";")
                     declared.update(new)
-            L += ["  " + x for x in (self.reaction32(r) if mixed else self.reaction64(r))]
+            body = self.reaction32(r) if mixed else self.reaction64(r)
+            if self.exp_noinline:
+                body = [x.replace("cgm::cg_exp_clamped(", "cgm::cg_exp_clamped_ool(").replace(
+                    "cgm::cg_exp(", "cgm::cg_exp_ool(") for x in body]
+            L += ["  " + x for x in body]
             if self.live_order:
                 done = [k for k in sorted(set(self.idx[sp] for sp in list(r.reactants) + list(r.products)))
                         if last[k] == p]
@@ -671,7 +677,7 @@ PRECISIONS = {"fp64": (True, False), "mixed": (False, True), "both": (True, True
 
 def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = None,
          sync_every: Optional[int] = None, precision: str = "both", tmem: Optional[bool] = None,
-         live_order: bool = True) -> str:
+         live_order: bool = True, exp_noinline: bool = False) -> str:
     """CUDA source of the mechanism's kernels: `precision` selects the FP64
     kernel, the mixed one or both; a mode without a generated kernel runs on
     the table-driven kernels."""
@@ -683,9 +689,11 @@ def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = Non
     tm64 = use_tmem(mech.ns, False) if tmem is None else tmem
     tm32 = use_tmem(mech.ns, True) if tmem is None else tmem
     em64 = _Emitter(mech, block or choose_block(mech.ns, False, tm64),
-                    SYNC_EVERY if sync_every is None else sync_every, tmem=tm64, live_order=live_order)
+                    SYNC_EVERY if sync_every is None else sync_every, tmem=tm64, live_order=live_order,
+                    exp_noinline=exp_noinline)
     em32 = _Emitter(mech, block or choose_block(mech.ns, True, tm32),
-                    SYNC_EVERY_MIXED if sync_every is None else sync_every, tmem=tm32, live_order=live_order)
+                    SYNC_EVERY_MIXED if sync_every is None else sync_every, tmem=tm32, live_order=live_order,
+                    exp_noinline=exp_noinline)
     ident = "".join(ch if ch.isalnum() else "_" for ch in (name or mech.name))
     src = [
         f"// Generated by chemgen_b200 (generate_chemistry.py --language cuda --precision {precision}) for mechanism '{mech.name}':",

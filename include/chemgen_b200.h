@@ -100,14 +100,17 @@ int chemgen_use_generated(chemgen_handle* h, int enable);
 int chemgen_kernel_kind(chemgen_handle* h, int mode);
 
 /* Analytic derivatives (no counterpart in the reference, whose torch
- * prototype chemgen/chemistry_nn.py:15-85 never ran); library-owned scratch
- * of 4*ns*ng doubles.
+ * prototype chemgen/chemistry_nn.py:15-85 never ran).
  * chemgen_jacobian: dense d wdot/d(T, Y) per point, J[(k*(ns+1) + c)*ng + i],
  *   column c = 0 for T, 1 + j for Y_j; precision 0 = double, 1 = float
- *   (FP64 rate evaluation, FP32 accumulation and storage of J).
+ *   (FP64 rate evaluation and accumulation, J stored in FP32).  Each row is
+ *   accumulated on chip and J is written once, with no scratch, when a
+ *   32-point tile's state and two rows fit in shared memory (up to ~180
+ *   species); larger mechanisms accumulate J in place with library-owned
+ *   scratch of 4*ns*ng doubles (FP32 accumulation for precision 1). 
  * chemgen_getrates_vjp: given G = dL/dwdot [ns*ng], the adjoint
  *   gT = dL/dT [ng], gY = dL/dY [ns*ng] and (if gP != NULL) gP = dL/dP [ng],
- *   without forming J. */
+ *   without forming J (library-owned scratch of 4*ns*ng doubles). */
 int chemgen_jacobian(chemgen_handle* h, int precision, const double* P, const double* T, int64_t ng,
                      const double* Y, void* J, void* stream);
 int chemgen_getrates_vjp(chemgen_handle* h, const double* P, const double* T, int64_t ng, const double* Y,
