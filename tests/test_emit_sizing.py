@@ -54,3 +54,55 @@ def test_tmem_option_for_the_mixed_kernel():
     assert src.count("cgg::tm_alloc") == 2
     mixed = src.split("cg_gen_mixed(", 1)[1]
     assert "sG[" not in mixed and "cgg::tm_ld(" in mixed
+
+
+@pytest.mark.parametrize("factory", [synthetic.gri_shape, synthetic.h2o2_10sp, synthetic.all_kinds])
+def test_live_range_order_is_a_permutation_that_shortens_live_ranges(factory):
+    mech = factory()
+    order = E.reaction_order(mech)
+    assert sorted(order) == list(range(mech.nr))
+    assert E.live_accumulators(mech, order) <= E.live_accumulators(mech, list(range(mech.nr)))
+    if mech.ns == 53:
+        assert E.live_accumulators(mech, order) <= 32
+
+
+def test_each_wdot_is_stored_once_after_its_last_reaction():
+    """Live-range mode: an accumulator is declared before the first reaction
+    that touches its species and stored right after the last one; species no
+    reaction touches are stored as zero; every species is stored once."""
+    mech = synthetic.gri_shape()
+    src = E.emit(mech, precision="fp64")
+    body = src.split("cg_gen_fp64(", 1)[1].split("\n}\n", 1)[0]
+    stores = re.findall(r"wdot\[\(int64_t\)(\d+) \* ng \+ i\] = (w\d+|0\.0);", body)
+    assert sorted(int(k) for k, _ in stores) == list(range(mech.ns))
+    for k, v in stores:
+        if v != "0.0":
+            assert v == f"w{k}"
+            decl = body.index(f" w{k} = 0.0")
+            last_use = max(body.rfind(f"w{k} += "), body.rfind(f"w{k} -= "), body.rfind(f"w{k} = fma("))
+            store = body.index(f"wdot[(int64_t){k} * ng + i] = w{k};")
+            assert decl < last_use < store
+
+
+@pytest.mark.slow
+def test_generated_53_species_kernels_fit_their_register_budget(tmp_path):
+    """ptxas's own register count and spills of the emitted 53-species
+    kernels (nvcc cross-compiles; no GPU): each fits the registers its
+    launch shape leaves per thread, with at most a few spilled words."""
+    import subprocess
+    from chemgen_b200.build import ARCH, FLAGS, nvcc
+    mech = synthetic.gri_shape()
+    src = tmp_path / "g.cu"
+    src.write_text(E.emit(mech))
+    r = subprocess.run([nvcc()] + ARCH + FLAGS + ["-I", E.os.path.join(E.HERE, "csrc"), "-Xptxas", "-v", "-c",
+                        str(src), "-o", str(tmp_path / "g.o")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    info = {}
+    for name, spill, regs in re.findall(r"Function properties for \w*?(cg_gen_\w+?)E.*?\n\s+\d+ bytes stack frame, "
+                                        r"(\d+) bytes spill stores.*?\nptxas info\s+: Used (\d+) registers", r.stderr):
+        info[name] = (int(regs), int(spill))
+    shapes = {"cg_gen_fp64": E.choose_block(53, False, True), "cg_gen_mixed": E.choose_block(53, True)}
+    assert set(info) == set(shapes), r.stderr[-2000:]
+    for name, (regs, spill) in info.items():
+        assert regs * shapes[name] <= E.REG_FILE, (name, regs)
+        assert spill <= 64, (name, spill)
