@@ -460,7 +460,7 @@ __global__ void __launch_bounds__(128) deriv_kernel(DevMech m, const double* __r
 // reaction is evaluated once per species it changes (about four times), in
 // exchange for J never being read back from memory.
 constexpr int kJTile = 32;
-constexpr int kJMaxWarps = 8;
+constexpr int kJMaxWarps = 16;
 
 template <typename JT>
 __global__ void __launch_bounds__(32 * kJMaxWarps, 1)

@@ -191,5 +191,46 @@ __device__ __forceinline__ void tm_ld(uint32_t a0, uint32_t a1, uint32_t a2, uin
     v3 = __hiloint2double((int)h3, (int)l3);
 }
 
+// Split form, so that the loads of the next reaction's values fly while this
+// reaction computes: tm_issue starts the load of one double into two 32-bit
+// registers without waiting; tm_wait_k completes every load issued so far
+// and takes the k pending pairs as in/out operands, so that no use of them
+// can be scheduled above it.
+__device__ __forceinline__ void tm_issue(uint32_t a, uint32_t& lo, uint32_t& hi) {
+    __syncwarp();
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(lo), "=r"(hi) : "r"(a));
+}
+__device__ __forceinline__ void tm_wait_1(uint32_t* r) {
+    __syncwarp();
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r[0]), "+r"(r[1])::"memory");
+}
+__device__ __forceinline__ void tm_wait_2(uint32_t* r) {
+    __syncwarp();
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3])::"memory");
+}
+__device__ __forceinline__ void tm_wait_3(uint32_t* r) {
+    __syncwarp();
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5])::"memory");
+}
+__device__ __forceinline__ void tm_wait_4(uint32_t* r) {
+    __syncwarp();
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]),
+                   "+r"(r[7])::"memory");
+}
+__device__ __forceinline__ void tm_wait_5(uint32_t* r) {
+    __syncwarp();
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]),
+                   "+r"(r[7]), "+r"(r[8]), "+r"(r[9])::"memory");
+}
+__device__ __forceinline__ void tm_wait_6(uint32_t* r) {
+    __syncwarp();
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]),
+                   "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11])::"memory");
+}
+
 }  // namespace cgg
 

@@ -43,6 +43,10 @@ namespace cg {
 constexpr int kTile = 128;       // points per CTA tile (TMEM lanes)
 constexpr int kChunk = 16;       // reactions per MMA chunk (MMA K)
 constexpr int kABytes = kTile * kChunk * 2;   // one BF16 A split tile
+constexpr int kNoExp = -100000;  // no nonzero rate yet
+constexpr int kTargetExp = 100;  // a group's first largest scaled rate lands near 2^100 ...
+constexpr int kMaxExp = 112;     // ... and none may pass 2^112 (sums stay below 2^127)
+constexpr int kMaxScale = 900;   // scale exponents stay inside FP64's exponent field
 
 // Pre-decoded record of a standard or three-body reaction with at most three
 // molecules per side (the common case), built once per plan on the device:
@@ -79,22 +83,19 @@ constexpr double kLog2eD = 1.4426950408889634074;
 constexpr float kLog2eF = 1.44269504f;
 constexpr float kLog10_2F = 0.30103000f;
 
-// 2^e for an integer e, applied in two FP32 steps so that large products
-// with small scales (and the reverse) keep their value.
-__device__ __forceinline__ float scale2(float m, int e) {
-    const int e1 = max(-126, min(e, 127));
-    const int e2 = max(-126, min(e - e1, 127));
-    return m * __int_as_float((e1 + 127) << 23) * __int_as_float((e2 + 127) << 23);
+// q = 2^a * prod * 2^eoff, a in FP64: 2^f of the fraction on the SFU times
+// the FP32 product, converted exactly to FP64, then 2^(n + eoff) in the FP64
+// exponent field.  The result keeps FP64's range: rates of progress span far
+// more than FP32's (at 300 K whole points sit below 2^-126 mol/cm^3/s).
+__device__ __forceinline__ double rate64(double a, float prod, int eoff) {
+    int n;
+    float f;
+    cgg::split2(a, n, f);
+    return (double)(cgg::ex2f(f) * prod) * cgg::exp2i(n + eoff);
 }
 
-// FP32 q = 2^a * prod * 2^eoff, a in FP64.
-__device__ __forceinline__ float rate32(double a, float prod, int eoff) {
-    const double magic = 6755399441055744.0;
-    const double t = a + magic;
-    const int n = __double2loint(t);
-    const float f = (float)(a - (t - magic));
-    return scale2(cgg::ex2f(f) * prod, n + eoff);
-}
+// Binary exponent of a nonzero finite double (floor(log2 |x|) for normal x).
+__device__ __forceinline__ int exponent_of(double x) { return ((__double2hiint(x) >> 20) & 0x7ff) - 1023; }
 
 struct TileCtx {
     const float* C;      // C * 2^32, stride kTile
@@ -103,41 +104,38 @@ struct TileCtx {
     float ctot32, Tf, invTf, lnT2f;
 };
 
-// log2 kf of a falloff reaction (Lindemann, Troe, SRI): FP64 exponents, FP32 blending.
+// log2 kf of a falloff reaction (Lindemann, Troe, SRI), in FP64 throughout
+// (troe.j2:9-45 in the log2 domain).  The FP32 blend that the 53-species
+// generated kernels use was measured on JetSurf 2.0 (382 Troe reactions,
+// several of them each point's dominant rate): its kf errors reached 5e-6,
+// mostly from FP32 exponent arguments in Fcent and the FP32 log10 Pr / f1 chain,
+// which put the normwise error of wdot at 7.6e-6 over 2^18 points.  In FP64
+// the blend costs about three exp and three log per falloff reaction.
 __device__ double falloff_l2(int kind, int flags, const DRxn& R, const DFall& f, double x2, float Ms,
                              const TileCtx& c) {
+    constexpr double kLog10_2 = 0.30102999566398119521, kLn2 = 0.69314718055994530942;
     const double ainf = (fma(R.b, c.lnT, R.lnA) - R.theta * c.invT) * kLog2eD;
     const double a0 = (fma(f.b0, c.lnT, f.lnA0) - f.theta0 * c.invT) * kLog2eD;
-    const double d = a0 - ainf;
-    const double magic = 6755399441055744.0;
-    const double t = d + magic;
-    int npr = __double2loint(t);
-    float mpr = cgg::ex2f((float)(d - (t - magic))) * Ms;
-    const int ex = ((__float_as_int(mpr) >> 23) & 0xff) - 126;
-    npr += ex - 32;
-    mpr = __int_as_float((__float_as_int(mpr) & 0x807fffff) | (126 << 23));   // [0.5, 1)
-    const float l2m = cgg::lg2f(mpr);
-    const float l2pr = (float)npr + l2m;
-    float l2r;
-    int nfix;
-    cgg::falloff_blend(mpr, npr, l2m, l2r, nfix);
-    float l2F = 0.0f;
+    const double M = (double)Ms * 2.3283064365386963e-10;   // Ms = M * 2^32
+    // log2 Pr and log2 Pr/(1 + Pr), without overflow at either end
+    const double l2pr = (a0 - ainf) + cgm::cg_log(M) * kLog2eD;
+    const double x = cgm::cg_exp_clamped(-fabs(l2pr) * kLn2);          // min(Pr, 1/Pr)
+    const double l2r = fmin(l2pr, 0.0) - cgm::cg_log(1.0 + x) * kLog2eD;
+    double l2F = 0.0;
     if (kind == CG_TROE) {
-        float Fc = fmaf((float)f.p[0], cgg::ex2f(-kLog2eF * c.Tf * (float)f.p[1]),
-                        (float)f.p[2] * cgg::ex2f(-kLog2eF * c.Tf * (float)f.p[3]));
-        if (flags & CG_F_TROE_T2) Fc += cgg::ex2f(-kLog2eF * (float)x2 * c.invTf);
-        const float lFc = kLog10_2F * cgg::lg2f(Fc);
-        const float lp = kLog10_2F * l2pr + fmaf(-0.67f, lFc, -0.4f);
-        const float f1 = __fdividef(lp, fmaf(-0.14f, lp, fmaf(-1.27f, lFc, 0.75f)));
-        l2F = __fdividef(lFc, fmaf(f1, f1, 1.0f)) / kLog10_2F;
+        double Fc = fma(f.p[0], cgm::cg_exp_clamped(-c.T * f.p[1]), f.p[2] * cgm::cg_exp_clamped(-c.T * f.p[3]));
+        if (flags & CG_F_TROE_T2) Fc += cgm::cg_exp_clamped(-x2 * c.invT);
+        const double lFc = cgm::cg_log10(Fc);
+        const double lp = fma(kLog10_2, l2pr, fma(-0.67, lFc, -0.4));
+        const double f1 = lp * cgm::cg_rcp(fma(-0.14, lp, fma(-1.27, lFc, 0.75)));
+        l2F = lFc * cgm::cg_rcp(fma(f1, f1, 1.0)) / kLog10_2;
     } else if (kind == CG_SRI) {
-        const float lp = kLog10_2F * l2pr;
-        const float X = __fdividef(1.0f, fmaf(lp, lp, 1.0f));
-        const float base = fmaf((float)f.p[0], cgg::ex2f(-kLog2eF * (float)f.p[1] * c.invTf),
-                                cgg::ex2f(-kLog2eF * c.Tf * (float)f.p[2]));
-        l2F = cgg::lg2f((float)f.p[3]) + fmaf(X, cgg::lg2f(base), (float)x2 * c.lnT2f);
+        const double lp = kLog10_2 * l2pr;
+        const double X = cgm::cg_rcp(fma(lp, lp, 1.0));
+        const double base = fma(f.p[0], cgm::cg_exp_clamped(-f.p[1] * c.invT), cgm::cg_exp_clamped(-c.T * f.p[2]));
+        l2F = (cgm::cg_log(f.p[3]) + fma(X, cgm::cg_log(base), x2 * c.lnT)) * kLog2eD;
     }
-    return ainf + ((double)nfix + (double)(l2r + l2F));
+    return ainf + (l2r + l2F);
 }
 
 // PLOG forward rate in FP64 (plog.j2:4-38).
@@ -168,7 +166,7 @@ __device__ double plog_kf64(const DevMech& m, int row, double P, double lnT, dou
 // FP64 evaluation of reaction r (PLOG, non-integer stoichiometry, falloff
 // with negative pre-exponential factors): kept out of line so that the
 // common FP32 path keeps few registers.
-__device__ __noinline__ float rate_of_progress_fp64(const DevMech& m, const DRxn& R, int kind, float Ms,
+__device__ __noinline__ double rate_of_progress_fp64(const DevMech& m, const DRxn& R, int kind, float Ms,
                                                     const TileCtx& c, int tid) {
     const bool compact = (R.flags & kFCompact) != 0;
     {
@@ -217,12 +215,12 @@ __device__ __noinline__ float rate_of_progress_fp64(const DevMech& m, const DRxn
         }
         double rr = qf - qb;
         if (kind == CG_THIRD_BODY) rr *= (double)Ms * cs;
-        return (float)rr;
+        return rr;
     }
 }
 
 // Net rate of progress of reaction r at point `tid` of the tile, FP32.
-__device__ float rate_of_progress(const DevMech& m, int r, const TileCtx& c, int tid) {
+__device__ double rate_of_progress(const DevMech& m, int r, const TileCtx& c, int tid) {
     const DRxn R = load_rxn(m.rxn + r);
     int kind = CG_STANDARD;
     while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
@@ -258,7 +256,7 @@ __device__ float rate_of_progress(const DevMech& m, int r, const TileCtx& c, int
         cf *= Ms;
         of += 1;
     }
-    float q = rate32(a, cf, -32 * of);
+    double q = rate64(a, cf, -32 * of);
     if (R.flags & CG_F_REVERSIBLE) {
         float cb = 1.0f;
         int ob = 0;
@@ -273,13 +271,13 @@ __device__ float rate_of_progress(const DevMech& m, int r, const TileCtx& c, int
             cb *= Ms;
             ob += 1;
         }
-        q -= rate32(a + g, cb, -32 * ob);
+        q -= rate64(a + g, cb, -32 * ob);
     }
     return sgn * q;
 }
 
 // Net rate of progress of a pre-decoded reaction (TcFast) at point `tid`, FP32.
-__device__ __forceinline__ float rate_fast(const DevMech& m, int r, const TcFast& F, const TileCtx& c, int tid) {
+__device__ __forceinline__ double rate_fast(const DevMech& m, int r, const TcFast& F, const TileCtx& c, int tid) {
     const double a = fma(F.b, c.lnT2, F.l2A) - F.th2 * c.invT;
     float Ms = 1.0f;
     if (F.flags & kFastThird) {
@@ -288,12 +286,12 @@ __device__ __forceinline__ float rate_fast(const DevMech& m, int r, const TcFast
             Ms = fmaf((float)__ldg(m.eff_val + e), c.C[__ldg(m.eff_sp + e) * kTile + tid], Ms);
     }
     const float cf = c.C[F.sr[0] * kTile + tid] * c.C[F.sr[1] * kTile + tid] * c.C[F.sr[2] * kTile + tid] * Ms;
-    float q = rate32(a, cf, -32 * (int)F.ordf);
+    double q = rate64(a, cf, -32 * (int)F.ordf);
     if (F.flags & kFastRev) {
         const double g = (c.G[F.sr[0] * kTile + tid] + c.G[F.sr[1] * kTile + tid] + c.G[F.sr[2] * kTile + tid]) -
                          (c.G[F.sp[0] * kTile + tid] + c.G[F.sp[1] * kTile + tid] + c.G[F.sp[2] * kTile + tid]);
         const float cb = c.C[F.sp[0] * kTile + tid] * c.C[F.sp[1] * kTile + tid] * c.C[F.sp[2] * kTile + tid] * Ms;
-        q -= rate32(a + g, cb, -32 * (int)F.ordb);
+        q -= rate64(a + g, cb, -32 * (int)F.ordb);
     }
     return (F.flags & kFastNeg) ? -q : q;
 }
@@ -434,7 +432,49 @@ __global__ void __launch_bounds__(kTile * NT, 1)
             sG[ns * kTile + pt] = 0.0;      // ... and no Gibbs term
         }
         __syncthreads();
+        // Per-point scale.  The rates of progress of one point span FP64's
+        // range, the MMA operands (BF16) and sums (FP32) only FP32's: each
+        // group of chunks accumulates 2^sc q with sc chosen, per point, from
+        // the first chunk holding a nonzero rate so that its largest lands
+        // at 2^kTargetExp.  A chunk whose scaled rates would pass 2^kMaxExp
+        // (headroom for sums of the mechanism's reactions) first ends the
+        // group for the whole tile; the FP64 flush divides by 2^sc.
         bool first_group = true;
+        int gpos = 0;                 // chunks issued in the current group
+        int sc = 0;                   // this point's scale exponent in the group
+        int smax = kNoExp;            // largest scaled exponent of the group so far
+        int* sMx = reinterpret_cast<int*>(sRed);   // [NT][128]; sRed is free after the prologue
+        auto flush = [&]() {
+            // end of a group of reactions: wait for its MMAs, then add the
+            // FP32 partial sums, unscaled, into the FP64 output; the NT warps
+            // that share a lane quadrant split the columns
+            for (int b = 0; b < 2; ++b)
+                if (pending[b]) {
+                    ok = um::mbar_wait(&mbar[b], parity[b]) && ok;
+                    parity[b] ^= 1u;
+                    pending[b] = false;
+                }
+            um::fence_after_sync();
+            if (ok) {
+                const double unscale = cgg::exp2i(-sc);
+                for (int col = 16 * (warp >> 2); col < npad; col += 16 * NT) {
+                    float v[16];
+                    um::tmem_ld16(um::tmem_lane_addr(tbase, warp & 3, col), v);
+                    if (act)
+                        for (int j = 0; j < 16; ++j)
+                            if (col + j < ns) {
+                                double* w = wdot + (int64_t)(col + j) * ng + i;
+                                const double x = (double)v[j] * unscale;
+                                *w = first_group ? x : *w + x;
+                            }
+                }
+            }
+            first_group = false;
+            gpos = 0;
+            smax = kNoExp;
+            um::fence_before_sync();
+            __syncthreads();
+        };
         for (int ch = 0; ch < nchunk && ok; ++ch) {
             const int buf = ch & 1;
             if (pending[buf]) {
@@ -447,16 +487,42 @@ __global__ void __launch_bounds__(kTile * NT, 1)
             const uint4* src = reinterpret_cast<const uint4*>(nu + (int64_t)ch * npad * kChunk);
             uint4* dst = reinterpret_cast<uint4*>(sB + buf * npad * 32);
             for (int q = tid; q < npad * 2; q += kTile * NT) dst[q] = __ldg(src + q);
-            // q for the chunk's reactions -> A operands (hi, mid, lo)
-            unsigned char* a0 = sA + buf * 3 * kABytes;
-            for (int j = sub; j < kChunk; j += NT) {
-                const int r = ch * kChunk + j;
-                float q = 0.0f;
-                if (r < m.nr) {
+            // this thread's reactions of the chunk: FP64 net rates of progress
+            constexpr int kPer = kChunk / NT;
+            double qv[kPer];
+            int emax = kNoExp;
+#pragma unroll
+            for (int jj = 0; jj < kPer; ++jj) {
+                const int r = ch * kChunk + sub + jj * NT;
+                double q = 0.0;
+                if (act && r < m.nr) {
                     const TcFast F = load_fast(fast + r);
                     q = (F.flags & kFastOn) ? rate_fast(m, r, F, c, pt) : rate_of_progress(m, r, c, pt);
                 }
-                if (!act) q = 0.0f;
+                qv[jj] = q;
+                if (q != 0.0) emax = max(emax, exponent_of(q));
+            }
+            sMx[sub * kTile + pt] = emax;
+            __syncthreads();
+            int ec = kNoExp;
+            for (int u = 0; u < NT; ++u) ec = max(ec, sMx[u * kTile + pt]);
+            const bool over = ec != kNoExp && smax != kNoExp && ec + sc > kMaxExp;
+            if (__syncthreads_or(over)) flush();
+            if (ec != kNoExp) {
+                if (smax == kNoExp) {
+                    sc = max(-kMaxScale, min(kMaxScale, kTargetExp - ec));
+                    smax = ec + sc;
+                } else {
+                    smax = max(smax, ec + sc);
+                }
+            }
+            // scaled and split exactly into three BF16 parts -> A operands
+            unsigned char* a0 = sA + buf * 3 * kABytes;
+            const double up = cgg::exp2i(sc);
+#pragma unroll
+            for (int jj = 0; jj < kPer; ++jj) {
+                const int j = sub + jj * NT;
+                const float q = (float)(qv[jj] * up);
                 const __nv_bfloat16 h = __float2bfloat16_rn(q);
                 const float r1 = q - __bfloat162float(h);
                 const __nv_bfloat16 md = __float2bfloat16_rn(r1);
@@ -469,7 +535,7 @@ __global__ void __launch_bounds__(kTile * NT, 1)
             um::fence_proxy_async();
             um::fence_before_sync();
             __syncthreads();
-            const bool group_start = (ch % group) == 0;
+            const bool group_start = gpos == 0;
             if (tid == 0) {
                 um::fence_after_sync();
                 const uint32_t bb = um::smem_addr(sB + buf * npad * 32);
@@ -483,33 +549,8 @@ __global__ void __launch_bounds__(kTile * NT, 1)
                 um::commit(&mbar[buf]);
             }
             pending[buf] = true;
-            if ((ch % group) == group - 1 || ch == nchunk - 1) {
-                // end of a group of reactions: wait for its MMAs, then add the
-                // FP32 partial sums into the FP64 output; the NT warps that
-                // share a lane quadrant split the columns
-                for (int b = 0; b < 2; ++b)
-                    if (pending[b]) {
-                        ok = um::mbar_wait(&mbar[b], parity[b]) && ok;
-                        parity[b] ^= 1u;
-                        pending[b] = false;
-                    }
-                um::fence_after_sync();
-                if (ok) {
-                    for (int col = 16 * (warp >> 2); col < npad; col += 16 * NT) {
-                        float v[16];
-                        um::tmem_ld16(um::tmem_lane_addr(tbase, warp & 3, col), v);
-                        if (act)
-                            for (int j = 0; j < 16; ++j)
-                                if (col + j < ns) {
-                                    double* w = wdot + (int64_t)(col + j) * ng + i;
-                                    *w = first_group ? (double)v[j] : *w + (double)v[j];
-                                }
-                    }
-                }
-                first_group = false;
-                um::fence_before_sync();
-                __syncthreads();
-            }
+            ++gpos;
+            if (gpos == group || ch == nchunk - 1) flush();
         }
         um::fence_before_sync();
         __syncthreads();

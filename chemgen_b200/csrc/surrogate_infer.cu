@@ -2,16 +2,15 @@
 // features -> 4 MLP layers -> decoded FP64 wdot in one kernel, activations
 // never leaving the SM.
 //
-// One persistent CTA of 640 threads per SM works through tiles of 128 points,
+// One persistent CTA of 384 threads per SM works through tiles of 128 points,
 // in two warp groups that run one tile apart:
-// * feature group (warps 16-19, one thread per point): the next tile's 64
+// * feature group (warps 8-11, one thread per point): the next tile's 64
 //   network inputs (1000/T, ln T, ln P/1 atm, ln X_k, zeros), centred and
 //   scaled, split into BF16 hi + lo parts, written into their own
 //   shared-memory A operand [128 x 128] (K-major canonical layout); then 128
 //   arrivals on the "features full" mbarrier.  It writes tile j+1 only after
 //   the first layer of tile j has consumed tile j ("features empty");
-// * compute group (warps 0-15, four per tensor-memory lane quadrant, each
-//   with a quarter of the columns): per layer one thread issues K/16 tcgen05.mma
+// * compute group (warps 0-7): per layer one thread issues K/16 tcgen05.mma
 //   (M = 128, N = 256 or 64, K = 16, BF16 in, FP32 accumulate in tensor
 //   memory) against the layer's weights, which a bulk asynchronous copy
 //   (cp.async.bulk, no multicast) brought into shared memory while the
@@ -39,7 +38,7 @@ namespace {
 
 using bf16 = __nv_bfloat16;
 
-constexpr int kPts = 128, kCompute = 512, kThreads = kCompute + kPts;
+constexpr int kPts = 128, kCompute = 256, kThreads = kCompute + kPts;
 constexpr int kDin = 64, kK1 = 2 * kDin, kHid = 256, kDout = 64;
 constexpr int kW1 = kHid * kK1, kW2 = kHid * kHid, kW4 = kDout * kHid;
 constexpr int kImgElems = kW1 + 2 * kW2 + kW4;
@@ -109,17 +108,16 @@ __device__ __forceinline__ bool write_features(unsigned char* sF, int row, int64
     const int64_t i = tile * kPts + row;
     const bool act = i < ng;
     const int64_t ic = act ? i : ng - 1;
-    // first pass over Y: the mixture sums (the second pass reads Y again
-    // through the caches, which keeps the register count low enough for
-    // sixteen compute warps beside this group)
+    float y[kDin - 3];
     double ysum = 0.0, ymin = 0.0;
-    float mix = 0.0f;
-#pragma unroll 8
-    for (int k = 0; k < ns; ++k) {
-        const double yd = __ldg(Y + (int64_t)k * ng + ic);
-        ysum += yd;
-        ymin = fmin(ymin, yd);
-        mix = fmaf(fmaxf((float)yd, 0.0f), (float)__ldg(inv_mw + k), mix);
+#pragma unroll
+    for (int k = 0; k < kDin - 3; ++k) {
+        const double yd = __ldg(Y + (int64_t)min(k, ns - 1) * ng + ic);
+        y[k] = (float)yd;
+        if (k < ns) {
+            ysum += yd;
+            ymin = fmin(ymin, yd);
+        }
     }
     const double t = __ldg(T + ic), pr = __ldg(P + ic);
     bool oob = false;
@@ -127,6 +125,10 @@ __device__ __forceinline__ bool write_features(unsigned char* sF, int row, int64
         oob = !(t >= __ldg(range) && t <= __ldg(range + 1) && pr >= __ldg(range + 2) && pr <= __ldg(range + 3) &&
                 ymin >= 0.0 && fabs(ysum - 1.0) < 1e-6);
     const float invT = (float)(1000.0 / t), lnT = logf((float)t), lnP = logf((float)(pr / 1013250.0));
+    float mix = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kDin - 3; ++k)
+        if (k < ns) mix = fmaf(fmaxf(y[k], 0.0f), (float)__ldg(inv_mw + k), mix);
     const float lmix = __logf(fmaxf(mix, 1e-37f));
 #pragma unroll
     for (int g = 0; g < kDin / 8; ++g) {
@@ -147,8 +149,7 @@ __device__ __forceinline__ bool write_features(unsigned char* sF, int row, int64
                         v = (lnP - nrm[4]) * nrm[5];
                     } else if (k < ns) {
                         // fast log: ~1e-5 absolute, below the ~2^-16 of the split inputs
-                        const float yk = (float)__ldg(Y + (int64_t)k * ng + ic);
-                        const float lx = __logf(fmaxf(yk, 1e-30f) * (float)__ldg(inv_mw + k)) - lmix;
+                        const float lx = __logf(fmaxf(y[k], 1e-30f) * (float)__ldg(inv_mw + k)) - lmix;
                         v = fminf(fmaxf((lx - nrm[6]) * nrm[7], -6.0f), 6.0f);
                     }
                 }
@@ -235,7 +236,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     } else {
         // ------------------------------------------------------ compute group
-        const int g4 = warp & 3, equart = warp >> 2;   // TMEM lane group, column quarter
+        const int g4 = warp & 3, ehalf = warp >> 2;   // TMEM lane group, column half
         const int erow = 32 * g4 + lane;
         const double lc = (double)__ldg(lnorm), ls = (double)__ldg(lnorm + 1);
         if (tid == 0) {
@@ -291,11 +292,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                     if (l < 3) {
                         const float* bl = bias + kHid * l;
 #pragma unroll 1
-                        for (int c = 64 * equart; c < 64 * equart + 64; c += 32) {
-                            uint32_t r[32];
-                            um::tmem_ld32(um::tmem_lane_addr(tbase, g4, c), r);
+                        for (int c = 128 * ehalf; c < 128 * ehalf + 128; c += 64) {
+                            uint32_t r[64];
+                            um::tmem_ld64(um::tmem_lane_addr(tbase, g4, c), r);
 #pragma unroll
-                            for (int q = 0; q < 2; ++q)
+                            for (int q = 0; q < 4; ++q)
                                 gelu_store16(r + 16 * q, bl + c + 16 * q, sA + um::kmajor_offset(erow, c + 16 * q, kHid),
                                              sA + um::kmajor_offset(erow, c + 16 * q + 8, kHid));
                         }
@@ -313,7 +314,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                             if (cL + q == ns) L = v[q];
                         const double scale = exp(lc + ls * (double)(L + __ldg(b4 + ns)));
 #pragma unroll 1
-                        for (int c = 16 * equart; c < 16 * equart + 16; c += 16) {
+                        for (int c = 32 * ehalf; c < 32 * ehalf + 32; c += 16) {
                             um::tmem_ld16(um::tmem_lane_addr(tbase, g4, c), v);
                             if (act) {
 #pragma unroll
