@@ -366,6 +366,19 @@ __global__ void __launch_bounds__(B) getrates_fp64_global(DevMech m, const doubl
 // written once per point, and nothing is kept in global scratch: DRAM traffic
 // is the inputs and outputs.
 
+// Pre-decoded record of a standard or three-body reaction with at most three
+// molecules a side, built once per mechanism: the rate needs no decoding,
+// no loop and no power; unused molecule slots name the dummy species ns,
+// whose C and EGp are 1.
+struct __align__(16) StFast {
+    double lnA, b, theta;        // ln|A|, b, Ea/Rc
+    unsigned short sr[3], sp[3]; // reactant / product molecules
+    unsigned int flags;          // kStOn | kStRev | kStThird | kStNeg
+    int pad[2];
+};
+static_assert(sizeof(StFast) == 48, "StFast must stay 48 bytes");
+constexpr unsigned kStOn = 1, kStRev = 2, kStThird = 4, kStNeg = 8;
+
 struct StagedPlan {
     int W = 16;                 // warps per CTA
     int kpw = 0;                // accumulator slots per warp (template instance)
@@ -376,22 +389,34 @@ struct StagedPlan {
     const int* ptr = nullptr;   // [nchunk][ns + 1] into the entries
     const int* er = nullptr;    // reaction of each entry, within its chunk
     const double* enu = nullptr;  // net stoichiometric coefficient of each entry
+    const StFast* fast = nullptr;   // [nr]
     void* dbuf = nullptr;
 };
 
 constexpr int kStTile = 32;
 
+__device__ __forceinline__ StFast load_stfast(const StFast* p) {
+    const int4* q = reinterpret_cast<const int4*>(p);
+    StFast f;
+    int4* d = reinterpret_cast<int4*>(&f);
+    d[0] = __ldg(q);
+    d[1] = __ldg(q + 1);
+    d[2] = __ldg(q + 2);
+    return f;
+}
+
 template <int W, int KPW>
 __global__ void __launch_bounds__(32 * W, 1)
     getrates_fp64_staged(DevMech m, int R, int nchunk, const int* __restrict__ cptr, const int* __restrict__ cer,
-                         const double* __restrict__ cnu, const double* __restrict__ P, const double* __restrict__ Tg,
+                         const double* __restrict__ cnu, const StFast* __restrict__ fast,
+                         const double* __restrict__ P, const double* __restrict__ Tg,
                          const double* __restrict__ Y, double* __restrict__ wdot, int64_t ng) {
     extern __shared__ double smem[];
     const int ns = m.ns;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double* sC = smem;                       // [ns][32]
-    double* sE = sC + ns * kStTile;          // [ns][32]
-    double* sQ = sE + ns * kStTile;          // [R][32]
+    double* sC = smem;                       // [ns + 1][32] (row ns: the dummy species, 1)
+    double* sE = sC + (ns + 1) * kStTile;    // [ns + 1][32]
+    double* sQ = sE + (ns + 1) * kStTile;    // [R][32]
     double* sRed = sQ + R * kStTile;         // [W][32]
     const int64_t ntiles = (ng + kStTile - 1) / kStTile;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -426,6 +451,10 @@ __global__ void __launch_bounds__(32 * W, 1)
         const double pfac = kPatm / (kR0 * T);
         for (int k = warp; k < ns; k += W)
             sE[k * kStTile + lane] = cgm::cg_exp_clamped(species_smh(m.thermo, k, T, pt.lnT, pt.invT)) * pfac;
+        if (warp == 0) {
+            sC[ns * kStTile + lane] = 1.0;
+            sE[ns * kStTile + lane] = 1.0;
+        }
         __syncthreads();                     // csum read by every warp before sRed is reused
         sRed[warp * kStTile + lane] = part;
         __syncthreads();
@@ -443,7 +472,24 @@ __global__ void __launch_bounds__(32 * W, 1)
             for (int rl = warp; rl < R; rl += W) {
                 const int r = c * R + rl;
                 double q = 0.0;
-                if (r < m.nr) {
+                const StFast F = load_stfast(fast + (r < m.nr ? r : 0));
+                if (r < m.nr && (F.flags & kStOn)) {
+                    const double kf = cgm::cg_exp_clamped(fma(F.b, pt.lnT, F.lnA) - F.theta * pt.invT);
+                    q = kf * C[F.sr[0] * kStTile] * C[F.sr[1] * kStTile] * C[F.sr[2] * kStTile];
+                    if (F.flags & kStRev) {
+                        const double num = E[F.sr[0] * kStTile] * E[F.sr[1] * kStTile] * E[F.sr[2] * kStTile];
+                        const double den = E[F.sp[0] * kStTile] * E[F.sp[1] * kStTile] * E[F.sp[2] * kStTile];
+                        q -= kf * num * rcp_nr(den) * C[F.sp[0] * kStTile] * C[F.sp[1] * kStTile] *
+                             C[F.sp[2] * kStTile];
+                    }
+                    if (F.flags & kStThird) {
+                        double M = ctot;
+                        for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
+                            M = fma(__ldg(m.eff_val + e), C[__ldg(m.eff_sp + e) * kStTile], M);
+                        q *= M;
+                    }
+                    if (F.flags & kStNeg) q = -q;
+                } else if (r < m.nr) {
                     const DRxn Rx = load_rxn(m.rxn + r);
                     int kind = CG_STANDARD;
                     while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
@@ -518,7 +564,7 @@ cudaError_t staged_prepare(const DevMech& m, const cg_mech_view& v, int device, 
     cudaError_t e = cudaGetDeviceProperties(&prop, device);
     if (e != cudaSuccess) return e;
     const size_t limit = prop.sharedMemPerBlockOptin;
-    const size_t fixed = (size_t)2 * ns * kStTile * 8 + (size_t)pl.W * kStTile * 8;
+    const size_t fixed = (size_t)2 * (ns + 1) * kStTile * 8 + (size_t)pl.W * kStTile * 8;
     if (fixed + (size_t)pl.W * kStTile * 8 > limit) return cudaErrorNotSupported;
     int R = (int)((limit - fixed) / (kStTile * 8));
     R = std::min(R, 256) / pl.W * pl.W;
@@ -566,16 +612,51 @@ cudaError_t staged_prepare(const DevMech& m, const cg_mech_view& v, int device, 
             cp[k + 1] = (int)er.size();
         }
     }
+    // fast records: standard and three-body reactions, integer stoichiometry,
+    // at most three molecules a side, A != 0
+    const double* karh = (const double*)v.a[CG_KARH];
+    const double* arh = (const double*)v.a[CG_ARH];
+    const int32_t* rflags = (const int32_t*)v.a[CG_FLAGS];
+    const int n_std = (int)v.s[CG_S_NSTD], n_3b = (int)v.s[CG_S_N3B];
+    std::vector<StFast> fr(nr);
+    for (int r = 0; r < nr; ++r) {
+        StFast f{};
+        f.lnA = karh[4 * r];
+        f.b = karh[4 * r + 1];
+        f.theta = karh[4 * r + 2];
+        for (int j = 0; j < 3; ++j) f.sr[j] = f.sp[j] = (unsigned short)ns;
+        bool ok = r < n_std + n_3b && arh[3 * r] != 0.0 && (rflags[r] & CG_F_INT_NU);
+        int nf = 0, nb = 0;
+        for (int j = rp[r]; ok && j < rp[r + 1]; ++j)
+            for (int k = 0; k < (int)rnu[j]; ++k) {
+                if (nf == 3) ok = false;
+                else f.sr[nf++] = (unsigned short)rsp[j];
+            }
+        for (int j = pp[r]; ok && j < pp[r + 1]; ++j)
+            for (int k = 0; k < (int)pnu[j]; ++k) {
+                if (nb == 3) ok = false;
+                else f.sp[nb++] = (unsigned short)psp[j];
+            }
+        if (ok)
+            f.flags = kStOn | ((rflags[r] & CG_F_REVERSIBLE) ? kStRev : 0) | (r >= n_std ? kStThird : 0) |
+                      (karh[4 * r + 3] < 0.0 ? kStNeg : 0);
+        else
+            f.flags = 0;
+        fr[r] = f;
+    }
     const size_t b_ptr = (ptr.size() * sizeof(int) + 255) / 256 * 256;
     const size_t b_er = (std::max<size_t>(er.size(), 1) * sizeof(int) + 255) / 256 * 256;
-    const size_t b_nu = std::max<size_t>(enu.size(), 1) * sizeof(double);
+    const size_t b_nu = (std::max<size_t>(enu.size(), 1) * sizeof(double) + 255) / 256 * 256;
+    const size_t b_fast = (size_t)nr * sizeof(StFast);
     StagedPlan* p = new StagedPlan(pl);
-    e = cudaMalloc(&p->dbuf, b_ptr + b_er + b_nu);
+    e = cudaMalloc(&p->dbuf, b_ptr + b_er + b_nu + b_fast);
     char* d = (char*)p->dbuf;
     if (e == cudaSuccess) e = cudaMemcpy(d, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !er.empty()) e = cudaMemcpy(d + b_ptr, er.data(), er.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !enu.empty())
         e = cudaMemcpy(d + b_ptr + b_er, enu.data(), enu.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d + b_ptr + b_er + b_nu, fr.data(), b_fast, cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(staged_kernel(p->kpw), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem);
     if (e != cudaSuccess) {
@@ -586,6 +667,7 @@ cudaError_t staged_prepare(const DevMech& m, const cg_mech_view& v, int device, 
     p->ptr = (const int*)d;
     p->er = (const int*)(d + b_ptr);
     p->enu = (const double*)(d + b_ptr + b_er);
+    p->fast = (const StFast*)(d + b_ptr + b_er + b_nu);
     p->grid = prop.multiProcessorCount;
     *out = p;
     return cudaSuccess;
@@ -604,8 +686,8 @@ cudaError_t launch_getrates_staged(const StagedPlan* p, const DevMech& m, const 
     const unsigned grid = (unsigned)std::min<int64_t>(tiles, p->grid);
     const unsigned threads = 32u * (unsigned)p->W;
 #define CG_STAGED_LAUNCH(K)                                                                                  \
-    getrates_fp64_staged<16, K><<<grid, threads, p->smem, s>>>(m, p->R, p->nchunk, p->ptr, p->er, p->enu, P, T, \
-                                                               Y, wdot, ng)
+    getrates_fp64_staged<16, K><<<grid, threads, p->smem, s>>>(m, p->R, p->nchunk, p->ptr, p->er, p->enu, p->fast, \
+                                                               P, T, Y, wdot, ng)
     switch (p->kpw) {
         case 8: CG_STAGED_LAUNCH(8); break;
         case 16: CG_STAGED_LAUNCH(16); break;
