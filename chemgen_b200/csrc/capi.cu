@@ -38,8 +38,10 @@ size_t deriv_workspace_bytes(int ns, int64_t ng);
 struct JacPlan;
 cudaError_t jac_prepare(const DevMech& m, const cg_mech_view& v, int device, JacPlan** out);
 void jac_release(JacPlan* p);
+size_t jac_rows_workspace_bytes(const JacPlan* p, const DevMech& m, int64_t ng);
 cudaError_t launch_jacobian_rows(const JacPlan* p, const DevMech& m, int precision, const double* P, const double* T,
-                                 const double* Y, void* J, int64_t ng, cudaStream_t s);
+                                 const double* Y, void* J, int64_t ng, double* scratch, size_t scratch_bytes,
+                                 cudaStream_t s);
 cudaError_t launch_jacobian(const DevMech& m, int precision, const double* P, const double* T, const double* Y,
                             void* J, int64_t ng, double* scratch, int sm_count, cudaStream_t s);
 cudaError_t launch_vjp(const DevMech& m, const double* P, const double* T, const double* Y, const double* G, double* gT,
@@ -539,9 +541,13 @@ int chemgen_jacobian(chemgen_handle* h, int precision, const double* P, const do
     if (precision != 0 && precision != 1) return CHEMGEN_ERR_INVALID_ARGUMENT;
     DeviceGuard g(h->device);
     if (h->max_side > 16) return CHEMGEN_ERR_UNSUPPORTED;
-    if (h->jac)
-        return status_of(cg::launch_jacobian_rows(h->jac, h->m, precision, P, T, Y, J, ng, (cudaStream_t)stream));
     std::lock_guard<std::mutex> lk(h->mu);
+    if (h->jac) {
+        st = ensure_ws_locked(h, cg::jac_rows_workspace_bytes(h->jac, h->m, ng));
+        if (st) return st;
+        return status_of(cg::launch_jacobian_rows(h->jac, h->m, precision, P, T, Y, J, ng, (double*)h->ws,
+                                                  h->ws_bytes, (cudaStream_t)stream));
+    }
     st = ensure_ws_locked(h, cg::deriv_workspace_bytes(h->ns, ng));
     if (st) return st;
     return status_of(cg::launch_jacobian(h->m, precision, P, T, Y, J, ng, (double*)h->ws, h->sm_count,

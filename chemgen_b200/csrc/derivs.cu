@@ -230,16 +230,18 @@ struct RxnGradT {
 };
 using RxnGrad = RxnGradT<16>;
 
-// NMAX = 3: compact reactions only (the caller checks kFCompact).
-template <int NMAX>
-__device__ __forceinline__ void reaction_grad(const DevMech& m, int r, const DRxn& R, const PointT& pt, double ctot,
-                                              double Pv, double lnP, const DState& st, SideT<NMAX>& re,
-                                              SideT<NMAX>& pr, RxnGradT<NMAX>& g) {
-    int kind = CG_STANDARD;
-    while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
-    if constexpr (NMAX == 3) load_sides3(R, re, pr);
-    else load_sides(m, R, re, pr);
-    double M = 0.0, kf, dlkf, gM = 0.0, dlkf_lnP = 0.0;
+// The rate constants of reaction r at one point: kf and its d ln kf/dT,
+// kb, and for three-body and falloff reactions M and d ln kf/dM (gM).  The
+// row-owner Jacobian computes them once per reaction and tile (KC = 5
+// values, stride 32 apart, in `kc`); reaction_grad can take them from there.
+constexpr int kKC = 5;   // kf, kb, dlkf, gM, M
+
+__device__ __forceinline__ void reaction_k(const DevMech& m, int r, const DRxn& R, int kind, const PointT& pt,
+                                           double ctot, double Pv, double lnP, const DState& st, double& kf,
+                                           double& kb, double& dlkf, double& gM, double& M, double& dlkf_lnP) {
+    M = 0.0;
+    gM = 0.0;
+    dlkf_lnP = 0.0;
     if (kind != CG_STANDARD && kind != CG_PLOG) {
         M = ctot;
         for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
@@ -254,6 +256,46 @@ __device__ __forceinline__ void reaction_grad(const DevMech& m, int r, const DRx
         const DFall f = load_fall(m.fall + R.aux);
         falloff_d(kind, R.flags, R, f, __ldg(&m.fall2[R.aux].T2), M, pt, kf, dlkf, gM);
     }
+    kb = 0.0;
+    if (R.flags & CG_F_REVERSIBLE) {
+        double num = 1.0, den = 1.0;
+        if (R.flags & kFCompact) {
+#pragma unroll
+            for (int j = 0; j < kMaxCompact; ++j) {
+                if (j < R.nre) num *= ipow3(st.E[slot_species(R.sp[j]) * st.s], slot_nu(R.sp[j]));
+                if (j < R.npr) den *= ipow3(st.E[slot_species(R.sp[3 + j]) * st.s], slot_nu(R.sp[3 + j]));
+            }
+        } else {
+            const int g = R.gen;
+            for (int j = __ldg(m.gen_rptr + g); j < __ldg(m.gen_rptr + g + 1); ++j)
+                num *= powi(st.E[__ldg(m.gen_sp + j) * st.s], __ldg(m.gen_nu + j));
+            for (int j = __ldg(m.gen_pptr + g); j < __ldg(m.gen_pptr + g + 1); ++j)
+                den *= powi(st.E[__ldg(m.gen_sp + j) * st.s], __ldg(m.gen_nu + j));
+        }
+        kb = kf * num * cgm::cg_rcp(den);
+    }
+}
+
+// NMAX = 3: compact reactions only (the caller checks kFCompact).  With
+// CACHED the rate constants come from kc (reaction_k's values).
+template <int NMAX, bool CACHED = false>
+__device__ __forceinline__ void reaction_grad(const DevMech& m, int r, const DRxn& R, const PointT& pt, double ctot,
+                                              double Pv, double lnP, const DState& st, SideT<NMAX>& re,
+                                              SideT<NMAX>& pr, RxnGradT<NMAX>& g, const double* kc = nullptr) {
+    int kind = CG_STANDARD;
+    while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
+    if constexpr (NMAX == 3) load_sides3(R, re, pr);
+    else load_sides(m, R, re, pr);
+    double M, kf, kb_c, dlkf, gM, dlkf_lnP = 0.0;
+    if constexpr (CACHED) {
+        kf = kc[0];
+        kb_c = kc[32];
+        dlkf = kc[64];
+        gM = kc[96];
+        M = kc[128];
+    } else {
+        reaction_k(m, r, R, kind, pt, ctot, Pv, lnP, st, kf, kb_c, dlkf, gM, M, dlkf_lnP);
+    }
     double cr[NMAX], cp[NMAX];
     double pf = 1.0;
 #pragma unroll(NMAX == 3 ? 3 : 1)
@@ -265,22 +307,18 @@ __device__ __forceinline__ void reaction_grad(const DevMech& m, int r, const DRx
     const double qf = kf * pf;
     double kb = 0.0, qb = 0.0, dlKc = 0.0;
     if (R.flags & CG_F_REVERSIBLE) {
-        double num = 1.0, den = 1.0, pb_ = 1.0;
+        double pb_ = 1.0;
 #pragma unroll(NMAX == 3 ? 3 : 1)
         for (int j = 0; j < NMAX; ++j)
-            if (j < re.n) {
-                num *= powi(st.E[re.sp[j] * st.s], re.nu[j]);
-                dlKc = fma(re.nu[j], st.D[re.sp[j] * st.s], dlKc);
-            }
+            if (j < re.n) dlKc = fma(re.nu[j], st.D[re.sp[j] * st.s], dlKc);
 #pragma unroll(NMAX == 3 ? 3 : 1)
         for (int j = 0; j < NMAX; ++j)
             if (j < pr.n) {
                 cp[j] = st.C[pr.sp[j] * st.s];
-                den *= powi(st.E[pr.sp[j] * st.s], pr.nu[j]);
                 pb_ *= powi(cp[j], pr.nu[j]);
                 dlKc = fma(-pr.nu[j], st.D[pr.sp[j] * st.s], dlKc);
             }
-        kb = kf * num * cgm::cg_rcp(den);
+        kb = kb_c;
         qb = kb * pb_;
     }
     const double mfac = (kind == CG_THIRD_BODY) ? M : 1.0;
@@ -460,13 +498,13 @@ __global__ void __launch_bounds__(128) deriv_kernel(DevMech m, const double* __r
 // reaction is evaluated once per species it changes (about four times), in
 // exchange for J never being read back from memory.
 constexpr int kJTile = 32;
-constexpr int kJMaxWarps = 16;
+constexpr int kJMaxWarps = 8;
 
 template <typename JT>
 __global__ void __launch_bounds__(32 * kJMaxWarps, 1)
     jac_rows_kernel(DevMech m, const int* __restrict__ lptr, const int* __restrict__ lrx,
                     const double* __restrict__ lnu, const double* __restrict__ P, const double* __restrict__ Tg,
-                    const double* __restrict__ Y, JT* __restrict__ J, int64_t ng) {
+                    const double* __restrict__ Y, JT* __restrict__ J, int64_t ng, double* __restrict__ kcache) {
     extern __shared__ double smem[];
     const int ns = m.ns, ncol = ns + 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -519,6 +557,23 @@ __global__ void __launch_bounds__(32 * kJMaxWarps, 1)
         const double lnP = cgm::cg_log(Pv);
         const DState st{sC + lane, sE + lane, sD + lane, nullptr, kJTile};
         const double iS = 1.0 / S;
+        // phase 1: every reaction's rate constants once, into this CTA's
+        // slice [nr][kKC][32] (a few hundred KB: it stays in L2)
+        double* kc = kcache + (int64_t)blockIdx.x * m.nr * kKC * kJTile;
+        for (int r = warp; r < m.nr; r += nw) {
+            const DRxn R = load_rxn(m.rxn + r);
+            int kind = CG_STANDARD;
+            while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
+            double kf, kb, dlkf, gM, M, dlp;
+            reaction_k(m, r, R, kind, pt, ctot, Pv, lnP, st, kf, kb, dlkf, gM, M, dlp);
+            double* o = kc + (int64_t)r * kKC * kJTile + lane;
+            o[0] = kf;
+            o[32] = kb;
+            o[64] = dlkf;
+            o[96] = gM;
+            o[128] = M;
+        }
+        __syncthreads();
         for (int k = warp; k < ns; k += nw) {
             for (int c = 0; c < ncol; ++c) row[c * kJTile] = 0.0;
             double ak = 0.0;
@@ -529,10 +584,11 @@ __global__ void __launch_bounds__(32 * kJMaxWarps, 1)
                 const DRxn R = load_rxn(m.rxn + r);
                 double dqdT, dqdM;
                 bool usesM;
+                const double* kr = kc + (int64_t)r * kKC * kJTile + lane;
                 if (R.flags & kFCompact) {
                     SideT<3> re, pr;
                     RxnGradT<3> g;
-                    reaction_grad<3>(m, r, R, pt, ctot, Pv, lnP, st, re, pr, g);
+                    reaction_grad<3, true>(m, r, R, pt, ctot, Pv, lnP, st, re, pr, g, kr);
 #pragma unroll
                     for (int j = 0; j < 6; ++j) row[(1 + g.dsp[j]) * kJTile] = fma(nu, g.dqc[j], row[(1 + g.dsp[j]) * kJTile]);
                     dqdT = g.dqdT;
@@ -541,7 +597,7 @@ __global__ void __launch_bounds__(32 * kJMaxWarps, 1)
                 } else {
                     Side re, pr;
                     RxnGrad g;
-                    reaction_grad<16>(m, r, R, pt, ctot, Pv, lnP, st, re, pr, g);
+                    reaction_grad<16, true>(m, r, R, pt, ctot, Pv, lnP, st, re, pr, g, kr);
                     for (int j = 0; j < g.nd; ++j)
                         row[(1 + g.dsp[j]) * kJTile] = fma(nu, g.dqc[j], row[(1 + g.dsp[j]) * kJTile]);
                     dqdT = g.dqdT;
@@ -660,16 +716,26 @@ void jac_release(JacPlan* p) {
     delete p;
 }
 
+size_t jac_rows_workspace_bytes(const JacPlan* p, const DevMech& m, int64_t ng) {
+    const int64_t tiles = (ng + kJTile - 1) / kJTile;
+    const int64_t grid = std::min<int64_t>(tiles, p->grid);
+    return (size_t)grid * m.nr * kKC * kJTile * sizeof(double);
+}
+
 cudaError_t launch_jacobian_rows(const JacPlan* p, const DevMech& m, int precision, const double* P, const double* T,
-                                 const double* Y, void* J, int64_t ng, cudaStream_t s) {
+                                 const double* Y, void* J, int64_t ng, double* scratch, size_t scratch_bytes,
+                                 cudaStream_t s) {
     if (ng <= 0) return cudaSuccess;
     const int64_t tiles = (ng + kJTile - 1) / kJTile;
     const unsigned grid = (unsigned)std::min<int64_t>(tiles, p->grid);
+    if (!scratch || scratch_bytes < jac_rows_workspace_bytes(p, m, ng)) return cudaErrorInvalidValue;
     const unsigned threads = 32u * (unsigned)p->warps;
     if (precision == 0)
-        jac_rows_kernel<double><<<grid, threads, p->smem, s>>>(m, p->lptr, p->lrx, p->lnu, P, T, Y, (double*)J, ng);
+        jac_rows_kernel<double><<<grid, threads, p->smem, s>>>(m, p->lptr, p->lrx, p->lnu, P, T, Y, (double*)J, ng,
+                                                               scratch);
     else
-        jac_rows_kernel<float><<<grid, threads, p->smem, s>>>(m, p->lptr, p->lrx, p->lnu, P, T, Y, (float*)J, ng);
+        jac_rows_kernel<float><<<grid, threads, p->smem, s>>>(m, p->lptr, p->lrx, p->lnu, P, T, Y, (float*)J, ng,
+                                                              scratch);
     return cudaGetLastError();
 }
 

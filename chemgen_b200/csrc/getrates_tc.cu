@@ -43,10 +43,6 @@ namespace cg {
 constexpr int kTile = 128;       // points per CTA tile (TMEM lanes)
 constexpr int kChunk = 16;       // reactions per MMA chunk (MMA K)
 constexpr int kABytes = kTile * kChunk * 2;   // one BF16 A split tile
-constexpr int kNoExp = -100000;  // no nonzero rate yet
-constexpr int kTargetExp = 100;  // a group's first largest scaled rate lands near 2^100 ...
-constexpr int kMaxExp = 112;     // ... and none may pass 2^112 (sums stay below 2^127)
-constexpr int kMaxScale = 900;   // scale exponents stay inside FP64's exponent field
 
 // Pre-decoded record of a standard or three-body reaction with at most three
 // molecules per side (the common case), built once per plan on the device:
@@ -71,6 +67,9 @@ struct MixedPlan {
     int grid = 0;
     int group = 4;          // chunks accumulated in FP32 before the FP64 flush
     int nt = 1;             // threads per point (blockDim = 128 nt)
+    int hot = 0;            // species with FP64 accumulators in spare tensor-memory columns
+    int hot_every = 8;      // chunks between the hot species' FP64 flushes
+    const int* perm = nullptr;  // accumulator column -> species (-1: padding)
     void* dbuf = nullptr;
     const __nv_bfloat16* nu = nullptr;
     const TcFast* fast = nullptr;
@@ -83,19 +82,22 @@ constexpr double kLog2eD = 1.4426950408889634074;
 constexpr float kLog2eF = 1.44269504f;
 constexpr float kLog10_2F = 0.30103000f;
 
-// q = 2^a * prod * 2^eoff, a in FP64: 2^f of the fraction on the SFU times
-// the FP32 product, converted exactly to FP64, then 2^(n + eoff) in the FP64
-// exponent field.  The result keeps FP64's range: rates of progress span far
-// more than FP32's (at 300 K whole points sit below 2^-126 mol/cm^3/s).
-__device__ __forceinline__ double rate64(double a, float prod, int eoff) {
-    int n;
-    float f;
-    cgg::split2(a, n, f);
-    return (double)(cgg::ex2f(f) * prod) * cgg::exp2i(n + eoff);
+// 2^e for an integer e, applied in two FP32 steps so that large products
+// with small scales (and the reverse) keep their value.
+__device__ __forceinline__ float scale2(float m, int e) {
+    const int e1 = max(-126, min(e, 127));
+    const int e2 = max(-126, min(e - e1, 127));
+    return m * __int_as_float((e1 + 127) << 23) * __int_as_float((e2 + 127) << 23);
 }
 
-// Binary exponent of a nonzero finite double (floor(log2 |x|) for normal x).
-__device__ __forceinline__ int exponent_of(double x) { return ((__double2hiint(x) >> 20) & 0x7ff) - 1023; }
+// FP32 q = 2^a * prod * 2^eoff, a in FP64.
+__device__ __forceinline__ float rate32(double a, float prod, int eoff) {
+    const double magic = 6755399441055744.0;
+    const double t = a + magic;
+    const int n = __double2loint(t);
+    const float f = (float)(a - (t - magic));
+    return scale2(cgg::ex2f(f) * prod, n + eoff);
+}
 
 struct TileCtx {
     const float* C;      // C * 2^32, stride kTile
@@ -166,7 +168,7 @@ __device__ double plog_kf64(const DevMech& m, int row, double P, double lnT, dou
 // FP64 evaluation of reaction r (PLOG, non-integer stoichiometry, falloff
 // with negative pre-exponential factors): kept out of line so that the
 // common FP32 path keeps few registers.
-__device__ __noinline__ double rate_of_progress_fp64(const DevMech& m, const DRxn& R, int kind, float Ms,
+__device__ __noinline__ float rate_of_progress_fp64(const DevMech& m, const DRxn& R, int kind, float Ms,
                                                     const TileCtx& c, int tid) {
     const bool compact = (R.flags & kFCompact) != 0;
     {
@@ -215,12 +217,12 @@ __device__ __noinline__ double rate_of_progress_fp64(const DevMech& m, const DRx
         }
         double rr = qf - qb;
         if (kind == CG_THIRD_BODY) rr *= (double)Ms * cs;
-        return rr;
+        return (float)rr;
     }
 }
 
 // Net rate of progress of reaction r at point `tid` of the tile, FP32.
-__device__ double rate_of_progress(const DevMech& m, int r, const TileCtx& c, int tid) {
+__device__ float rate_of_progress(const DevMech& m, int r, const TileCtx& c, int tid) {
     const DRxn R = load_rxn(m.rxn + r);
     int kind = CG_STANDARD;
     while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
@@ -256,7 +258,7 @@ __device__ double rate_of_progress(const DevMech& m, int r, const TileCtx& c, in
         cf *= Ms;
         of += 1;
     }
-    double q = rate64(a, cf, -32 * of);
+    float q = rate32(a, cf, -32 * of);
     if (R.flags & CG_F_REVERSIBLE) {
         float cb = 1.0f;
         int ob = 0;
@@ -271,13 +273,13 @@ __device__ double rate_of_progress(const DevMech& m, int r, const TileCtx& c, in
             cb *= Ms;
             ob += 1;
         }
-        q -= rate64(a + g, cb, -32 * ob);
+        q -= rate32(a + g, cb, -32 * ob);
     }
     return sgn * q;
 }
 
 // Net rate of progress of a pre-decoded reaction (TcFast) at point `tid`, FP32.
-__device__ __forceinline__ double rate_fast(const DevMech& m, int r, const TcFast& F, const TileCtx& c, int tid) {
+__device__ __forceinline__ float rate_fast(const DevMech& m, int r, const TcFast& F, const TileCtx& c, int tid) {
     const double a = fma(F.b, c.lnT2, F.l2A) - F.th2 * c.invT;
     float Ms = 1.0f;
     if (F.flags & kFastThird) {
@@ -286,12 +288,12 @@ __device__ __forceinline__ double rate_fast(const DevMech& m, int r, const TcFas
             Ms = fmaf((float)__ldg(m.eff_val + e), c.C[__ldg(m.eff_sp + e) * kTile + tid], Ms);
     }
     const float cf = c.C[F.sr[0] * kTile + tid] * c.C[F.sr[1] * kTile + tid] * c.C[F.sr[2] * kTile + tid] * Ms;
-    double q = rate64(a, cf, -32 * (int)F.ordf);
+    float q = rate32(a, cf, -32 * (int)F.ordf);
     if (F.flags & kFastRev) {
         const double g = (c.G[F.sr[0] * kTile + tid] + c.G[F.sr[1] * kTile + tid] + c.G[F.sr[2] * kTile + tid]) -
                          (c.G[F.sp[0] * kTile + tid] + c.G[F.sp[1] * kTile + tid] + c.G[F.sp[2] * kTile + tid]);
         const float cb = c.C[F.sp[0] * kTile + tid] * c.C[F.sp[1] * kTile + tid] * c.C[F.sp[2] * kTile + tid] * Ms;
-        q -= rate64(a + g, cb, -32 * (int)F.ordb);
+        q -= rate32(a + g, cb, -32 * (int)F.ordb);
     }
     return (F.flags & kFastNeg) ? -q : q;
 }
@@ -354,7 +356,8 @@ __global__ void __launch_bounds__(kTile * NT, 1)
     getrates_tc_kernel(DevMech m, const __nv_bfloat16* __restrict__ nu, const TcFast* __restrict__ fast, int npad,
                        int nhalf, int nchunk, uint32_t tcols,
                        const double* __restrict__ P, const double* __restrict__ Tg, const double* __restrict__ Y,
-                       double* __restrict__ wdot, int64_t ng, double* __restrict__ gscratch, int* err, int group) {
+                       double* __restrict__ wdot, int64_t ng, double* __restrict__ gscratch, int* err, int group,
+                       const int* __restrict__ perm, int hot, int hot_every) {
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int pt = tid & (kTile - 1), sub = tid >> 7;          // point of the tile, share of its work
@@ -432,49 +435,8 @@ __global__ void __launch_bounds__(kTile * NT, 1)
             sG[ns * kTile + pt] = 0.0;      // ... and no Gibbs term
         }
         __syncthreads();
-        // Per-point scale.  The rates of progress of one point span FP64's
-        // range, the MMA operands (BF16) and sums (FP32) only FP32's: each
-        // group of chunks accumulates 2^sc q with sc chosen, per point, from
-        // the first chunk holding a nonzero rate so that its largest lands
-        // at 2^kTargetExp.  A chunk whose scaled rates would pass 2^kMaxExp
-        // (headroom for sums of the mechanism's reactions) first ends the
-        // group for the whole tile; the FP64 flush divides by 2^sc.
         bool first_group = true;
-        int gpos = 0;                 // chunks issued in the current group
-        int sc = 0;                   // this point's scale exponent in the group
-        int smax = kNoExp;            // largest scaled exponent of the group so far
-        int* sMx = reinterpret_cast<int*>(sRed);   // [NT][128]; sRed is free after the prologue
-        auto flush = [&]() {
-            // end of a group of reactions: wait for its MMAs, then add the
-            // FP32 partial sums, unscaled, into the FP64 output; the NT warps
-            // that share a lane quadrant split the columns
-            for (int b = 0; b < 2; ++b)
-                if (pending[b]) {
-                    ok = um::mbar_wait(&mbar[b], parity[b]) && ok;
-                    parity[b] ^= 1u;
-                    pending[b] = false;
-                }
-            um::fence_after_sync();
-            if (ok) {
-                const double unscale = cgg::exp2i(-sc);
-                for (int col = 16 * (warp >> 2); col < npad; col += 16 * NT) {
-                    float v[16];
-                    um::tmem_ld16(um::tmem_lane_addr(tbase, warp & 3, col), v);
-                    if (act)
-                        for (int j = 0; j < 16; ++j)
-                            if (col + j < ns) {
-                                double* w = wdot + (int64_t)(col + j) * ng + i;
-                                const double x = (double)v[j] * unscale;
-                                *w = first_group ? x : *w + x;
-                            }
-                }
-            }
-            first_group = false;
-            gpos = 0;
-            smax = kNoExp;
-            um::fence_before_sync();
-            __syncthreads();
-        };
+        int nhot = 0;                    // hot flushes so far in this tile
         for (int ch = 0; ch < nchunk && ok; ++ch) {
             const int buf = ch & 1;
             if (pending[buf]) {
@@ -487,42 +449,16 @@ __global__ void __launch_bounds__(kTile * NT, 1)
             const uint4* src = reinterpret_cast<const uint4*>(nu + (int64_t)ch * npad * kChunk);
             uint4* dst = reinterpret_cast<uint4*>(sB + buf * npad * 32);
             for (int q = tid; q < npad * 2; q += kTile * NT) dst[q] = __ldg(src + q);
-            // this thread's reactions of the chunk: FP64 net rates of progress
-            constexpr int kPer = kChunk / NT;
-            double qv[kPer];
-            int emax = kNoExp;
-#pragma unroll
-            for (int jj = 0; jj < kPer; ++jj) {
-                const int r = ch * kChunk + sub + jj * NT;
-                double q = 0.0;
-                if (act && r < m.nr) {
+            // q for the chunk's reactions -> A operands (hi, mid, lo)
+            unsigned char* a0 = sA + buf * 3 * kABytes;
+            for (int j = sub; j < kChunk; j += NT) {
+                const int r = ch * kChunk + j;
+                float q = 0.0f;
+                if (r < m.nr) {
                     const TcFast F = load_fast(fast + r);
                     q = (F.flags & kFastOn) ? rate_fast(m, r, F, c, pt) : rate_of_progress(m, r, c, pt);
                 }
-                qv[jj] = q;
-                if (q != 0.0) emax = max(emax, exponent_of(q));
-            }
-            sMx[sub * kTile + pt] = emax;
-            __syncthreads();
-            int ec = kNoExp;
-            for (int u = 0; u < NT; ++u) ec = max(ec, sMx[u * kTile + pt]);
-            const bool over = ec != kNoExp && smax != kNoExp && ec + sc > kMaxExp;
-            if (__syncthreads_or(over)) flush();
-            if (ec != kNoExp) {
-                if (smax == kNoExp) {
-                    sc = max(-kMaxScale, min(kMaxScale, kTargetExp - ec));
-                    smax = ec + sc;
-                } else {
-                    smax = max(smax, ec + sc);
-                }
-            }
-            // scaled and split exactly into three BF16 parts -> A operands
-            unsigned char* a0 = sA + buf * 3 * kABytes;
-            const double up = cgg::exp2i(sc);
-#pragma unroll
-            for (int jj = 0; jj < kPer; ++jj) {
-                const int j = sub + jj * NT;
-                const float q = (float)(qv[jj] * up);
+                if (!act) q = 0.0f;
                 const __nv_bfloat16 h = __float2bfloat16_rn(q);
                 const float r1 = q - __bfloat162float(h);
                 const __nv_bfloat16 md = __float2bfloat16_rn(r1);
@@ -535,7 +471,7 @@ __global__ void __launch_bounds__(kTile * NT, 1)
             um::fence_proxy_async();
             um::fence_before_sync();
             __syncthreads();
-            const bool group_start = gpos == 0;
+            const bool group_start = (ch % group) == 0;
             if (tid == 0) {
                 um::fence_after_sync();
                 const uint32_t bb = um::smem_addr(sB + buf * npad * 32);
@@ -549,8 +485,78 @@ __global__ void __launch_bounds__(kTile * NT, 1)
                 um::commit(&mbar[buf]);
             }
             pending[buf] = true;
-            ++gpos;
-            if (gpos == group || ch == nchunk - 1) flush();
+            const bool group_end = (ch % group) == group - 1 || ch == nchunk - 1;
+            if (hot > 0 && !group_end && (ch % hot_every) == hot_every - 1) {
+                // hot flush: the FP32 sums of the most-touched species (columns
+                // 0 .. hot-1) move into their FP64 accumulators (columns npad +
+                // 2j, +1) and restart from zero, so that FP32 never sums more
+                // than hot_every chunks of them; tensor-memory traffic only
+                for (int b = 0; b < 2; ++b)
+                    if (pending[b]) {
+                        ok = um::mbar_wait(&mbar[b], parity[b]) && ok;
+                        parity[b] ^= 1u;
+                        pending[b] = false;
+                    }
+                um::fence_after_sync();
+                if (ok) {
+                    for (int blk = warp >> 2; blk < hot / 16; blk += NT) {
+                        float v[16];
+                        uint32_t d[32];
+                        um::tmem_ld16(um::tmem_lane_addr(tbase, warp & 3, 16 * blk), v);
+                        if (nhot > 0) um::tmem_ld32(um::tmem_lane_addr(tbase, warp & 3, npad + 32 * blk), d);
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            const double a = (nhot > 0 ? __hiloint2double((int)d[2 * j + 1], (int)d[2 * j]) : 0.0) +
+                                             (double)v[j];
+                            d[2 * j] = (uint32_t)__double2loint(a);
+                            d[2 * j + 1] = (uint32_t)__double2hiint(a);
+                        }
+                        um::tmem_st32(um::tmem_lane_addr(tbase, warp & 3, npad + 32 * blk), d);
+                        uint32_t z[16];
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) z[j] = 0u;
+                        um::tmem_st16(um::tmem_lane_addr(tbase, warp & 3, 16 * blk), z);
+                    }
+                    um::tmem_wait_st();
+                }
+                ++nhot;
+                um::fence_before_sync();
+                __syncthreads();
+            }
+            if (group_end) {
+                // end of a group of reactions: wait for its MMAs, then add the
+                // FP32 partial sums into the FP64 output; the NT warps that
+                // share a lane quadrant split the columns
+                for (int b = 0; b < 2; ++b)
+                    if (pending[b]) {
+                        ok = um::mbar_wait(&mbar[b], parity[b]) && ok;
+                        parity[b] ^= 1u;
+                        pending[b] = false;
+                    }
+                um::fence_after_sync();
+                if (ok) {
+                    for (int col = 16 * (warp >> 2); col < npad; col += 16 * NT) {
+                        float v[16];
+                        uint32_t d[32];
+                        um::tmem_ld16(um::tmem_lane_addr(tbase, warp & 3, col), v);
+                        const bool h64 = col < hot && nhot > 0;
+                        if (h64) um::tmem_ld32(um::tmem_lane_addr(tbase, warp & 3, npad + 2 * col), d);
+                        if (act)
+                            for (int j = 0; j < 16; ++j) {
+                                const int sp = __ldg(perm + col + j);
+                                if (sp >= 0) {
+                                    double x = (double)v[j];
+                                    if (h64) x += __hiloint2double((int)d[2 * j + 1], (int)d[2 * j]);
+                                    double* w = wdot + (int64_t)sp * ng + i;
+                                    *w = first_group ? x : *w + x;
+                                }
+                            }
+                    }
+                }
+                first_group = false;
+                um::fence_before_sync();
+                __syncthreads();
+            }
         }
         um::fence_before_sync();
         __syncthreads();
@@ -572,7 +578,8 @@ cudaError_t launch_tc(const MixedPlan* p, const DevMech& m, const double* P, con
                       double* wdot, int64_t ng, double* scratch, int64_t grid, cudaStream_t s) {
     getrates_tc_kernel<GS, NT><<<(unsigned)grid, kTile * NT, p->smem, s>>>(m, p->nu, p->fast, p->npad, p->nhalf, p->nchunk,
                                                                            p->tcols, P, T, Y, wdot, ng, scratch,
-                                                                           p->err, p->group);
+                                                                           p->err, p->group, p->perm, p->hot,
+                                                                           p->hot_every);
     return cudaGetLastError();
 }
 
@@ -641,6 +648,19 @@ cudaError_t mixed_prepare(const DevMech& m, const cg_mech_view& v, int device, M
         for (int j = rp[r]; j < rp[r + 1]; ++j) nuf[(size_t)rsp[j] * nr + r] -= (float)rnu[j];
         for (int j = pp[r]; j < pp[r + 1]; ++j) nuf[(size_t)psp[j] * nr + r] += (float)pnu[j];
     }
+    // accumulator columns: for large mechanisms (one FP64 flush per tile) the
+    // species most reactions touch come first, and up to 48 of them (what the
+    // spare tensor-memory columns hold as FP64, in multiples of 16) get FP64
+    // accumulators flushed every hot_every chunks; otherwise file order
+    std::vector<int> perm(npad, -1);
+    for (int n = 0; n < ns; ++n) perm[n] = n;
+    if (p->group == nchunk && nchunk > p->hot_every) {
+        std::vector<int> nnz(ns, 0);
+        for (int n = 0; n < ns; ++n)
+            for (int r = 0; r < nr; ++r) nnz[n] += nuf[(size_t)n * nr + r] != 0.0f;
+        std::stable_sort(perm.begin(), perm.begin() + ns, [&](int a, int b) { return nnz[a] > nnz[b]; });
+        p->hot = std::min(48, std::min(((int)tcols - npad) / 2, ns) / 16 * 16);
+    }
     std::vector<__nv_bfloat16> img((size_t)nchunk * npad * kChunk, __float2bfloat16(0.0f));
     bool exact = true;
     for (int ch = 0; ch < nchunk; ++ch)
@@ -648,7 +668,7 @@ cudaError_t mixed_prepare(const DevMech& m, const cg_mech_view& v, int device, M
             for (int k = 0; k < kChunk; ++k) {
                 const int r = ch * kChunk + k;
                 if (r >= nr) continue;
-                const float x = nuf[(size_t)n * nr + r];
+                const float x = nuf[(size_t)perm[n] * nr + r];
                 const __nv_bfloat16 b = __float2bfloat16(x);
                 if (__bfloat162float(b) != x) exact = false;
                 const size_t off = ((size_t)(n >> 3) * (kChunk * 16) + (k >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2) / 2;
@@ -659,11 +679,15 @@ cudaError_t mixed_prepare(const DevMech& m, const cg_mech_view& v, int device, M
         return cudaErrorNotSupported;                  // coefficients not exact in BF16
     }
     const size_t img_bytes = (img.size() * sizeof(__nv_bfloat16) + 255) / 256 * 256;
-    const size_t fast_bytes = (size_t)nr * sizeof(TcFast);
-    const size_t bytes = img_bytes + fast_bytes + 256;
+    const size_t fast_bytes = ((size_t)nr * sizeof(TcFast) + 255) / 256 * 256;
+    const size_t perm_bytes = ((size_t)npad * sizeof(int) + 255) / 256 * 256;
+    const size_t bytes = img_bytes + fast_bytes + perm_bytes + 256;
     e = cudaMalloc(&p->dbuf, bytes);
     if (e == cudaSuccess) e = cudaMemcpy(p->dbuf, img.data(), img.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset((char*)p->dbuf + bytes - 256, 0, 256);
+    if (e == cudaSuccess)
+        e = cudaMemcpy((char*)p->dbuf + img_bytes + fast_bytes, perm.data(), perm.size() * sizeof(int),
+                       cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(kernel_for(p->g_smem, p->nt),
                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem);
     if (e != cudaSuccess) {
@@ -673,6 +697,7 @@ cudaError_t mixed_prepare(const DevMech& m, const cg_mech_view& v, int device, M
     }
     p->nu = (const __nv_bfloat16*)p->dbuf;
     p->fast = (const TcFast*)((char*)p->dbuf + img_bytes);
+    p->perm = (const int*)((char*)p->dbuf + img_bytes + fast_bytes);
     if (nr > 0) {
         build_fast_kernel<<<(nr + 127) / 128, 128>>>(m, (TcFast*)p->fast);
         e = cudaGetLastError();
