@@ -104,10 +104,12 @@ int chemgen_kernel_kind(chemgen_handle* h, int mode);
  * chemgen_jacobian: dense d wdot/d(T, Y) per point, J[(k*(ns+1) + c)*ng + i],
  *   column c = 0 for T, 1 + j for Y_j; precision 0 = double, 1 = float
  *   (FP64 rate evaluation and accumulation, J stored in FP32).  Each row is
- *   accumulated on chip and J is written once, with no scratch, when a
- *   32-point tile's state and two rows fit in shared memory (up to ~180
- *   species); larger mechanisms accumulate J in place with library-owned
- *   scratch of 4*ns*ng doubles (FP32 accumulation for precision 1). 
+ *   accumulated on chip and J is written once when a 32-point tile's state
+ *   and two rows fit in shared memory (up to ~180 species); the tile's rate
+ *   constants go to library-owned scratch of 5*nr*32 doubles per SM (about
+ *   60 MB at 325 reactions, resident in L2).  Larger mechanisms accumulate J
+ *   in place with library-owned scratch of 4*ns*ng doubles (FP32
+ *   accumulation for precision 1). 
  * chemgen_getrates_vjp: given G = dL/dwdot [ns*ng], the adjoint
  *   gT = dL/dT [ng], gY = dL/dY [ns*ng] and (if gP != NULL) gP = dL/dP [ng],
  *   without forming J (library-owned scratch of 4*ns*ng doubles). */
