@@ -29,6 +29,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "../../include/chemgen_b200.h"
@@ -41,6 +42,7 @@ using bf16 = __nv_bfloat16;
 
 constexpr int kTM = 128;    // rows per tile (MMA M, tensor-memory lanes)
 constexpr int kKC = 64;     // K per pipeline stage
+constexpr int kStages = 3;  // shared-memory stages (two chunks in flight beside the one computed)
 enum { kStore = 0, kStoreT = 1, kBiasGelu = 2, kBias = 3, kGeluBack = 4 };
 
 __device__ int g_mlp_tc_err = 0;
@@ -81,13 +83,16 @@ __global__ void __launch_bounds__(128) mlp_gemm_tc_kernel(TcArgs g) {
     constexpr int kBBytes = NT * kKC * 2;
     constexpr int kStage = kABytes + kBBytes;
     constexpr uint32_t kCols = NT < 32 ? 32u : (uint32_t)NT;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + 2 * kStage);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 2);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + kStages * kStage);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + kStages);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * kTM, n0 = blockIdx.y * NT;
+    // this CTA's share of K (split-K: blockIdx.z of gridDim.z, whole chunks)
+    const int nkc = g.K / kKC;
+    const int per = (nkc + gridDim.z - 1) / gridDim.z;
+    const int kc0 = blockIdx.z * per, kc1 = min(nkc, kc0 + per);
     if (tid == 0) {
-        um::mbar_init(&mbar[0], 1);
-        um::mbar_init(&mbar[1], 1);
+        for (int i = 0; i < kStages; ++i) um::mbar_init(&mbar[i], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) um::tmem_alloc(tslot, kCols);
@@ -96,16 +101,10 @@ __global__ void __launch_bounds__(128) mlp_gemm_tc_kernel(TcArgs g) {
     um::fence_after_sync();
     const uint32_t tbase = *tslot;
     const uint32_t idesc = um::idesc_bf16(kTM, NT);
-    uint32_t parity[2] = {0u, 0u};
+    uint32_t parity[kStages] = {};
     bool ok = true;
-    int it = 0;
-    for (int k0 = 0; k0 < g.K; k0 += kKC, ++it) {
-        const int st = it & 1;
-        if (it >= 2) {
-            // the MMAs that read this stage two chunks ago have finished
-            ok = um::mbar_wait(&mbar[st], parity[st]) && ok;
-            parity[st] ^= 1u;
-        }
+    auto load = [&](int kc, int st) {
+        const int k0 = kc * kKC;
         unsigned char* sA = sm + st * kStage;
         unsigned char* sB = sA + kABytes;
         for (int c = tid; c < kTM * 8; c += 128) {
@@ -116,12 +115,29 @@ __global__ void __launch_bounds__(128) mlp_gemm_tc_kernel(TcArgs g) {
             const int r = c >> 3, kk = (c & 7) * 8;
             cp_async16(sB + um::kmajor_offset(r, kk, kKC), g.B + (int64_t)(n0 + r) * g.ldb + k0 + kk);
         }
-        cp_async_wait_all();
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    // the copies of the next chunk fly while the tensor core works on this one
+    if (kc0 < kc1) load(kc0, 0);
+    for (int kc = kc0; kc < kc1; ++kc) {
+        const int it = kc - kc0, st = it % kStages;
+        if (kc + 1 < kc1) {
+            const int st1 = (it + 1) % kStages;
+            if (it + 1 >= kStages) {
+                // the MMAs that read stage st1 (chunk it + 1 - kStages) have finished
+                ok = um::mbar_wait(&mbar[st1], parity[st1]) && ok;
+                parity[st1] ^= 1u;
+            }
+            load(kc + 1, st1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
         um::fence_proxy_async();
         __syncthreads();
         if (tid == 0) {
             um::fence_after_sync();
-            const uint32_t a = um::smem_addr(sA), b = um::smem_addr(sB);
+            const uint32_t a = um::smem_addr(sm + st * kStage), b = um::smem_addr(sm + st * kStage + kABytes);
 #pragma unroll
             for (int ks = 0; ks < kKC / 16; ++ks)
                 um::mma_bf16(tbase, um::desc_kmajor(a, kKC, ks), um::desc_kmajor(b, kKC, ks), idesc,
@@ -129,15 +145,16 @@ __global__ void __launch_bounds__(128) mlp_gemm_tc_kernel(TcArgs g) {
             um::commit(&mbar[st]);
         }
     }
-    // the last (up to two) commits
-    for (int j = it >= 2 ? it - 2 : 0; j < it; ++j) {
-        const int st = j & 1;
+    // the commits not yet waited for (the last min(kStages, chunks) ones)
+    const int nit = kc1 - kc0;
+    for (int j = nit > kStages ? nit - kStages : 0; j < nit; ++j) {
+        const int st = j % kStages;
         ok = um::mbar_wait(&mbar[st], parity[st]) && ok;
         parity[st] ^= 1u;
     }
     um::fence_after_sync();
     const int m = m0 + 32 * warp + lane;
-    if (ok) {
+    if (ok && nit > 0) {
 #pragma unroll 1
         for (int c0 = 0; c0 < NT; c0 += 16) {
             float v[16];
@@ -147,12 +164,10 @@ __global__ void __launch_bounds__(128) mlp_gemm_tc_kernel(TcArgs g) {
             for (int j = 0; j < 16; ++j) {
                 const int n = nb + j;
                 float x = v[j];
-                if (g.epi == kStore) {
-                    float* c = g.C + (int64_t)m * g.ldc + n;
-                    *c = g.accumulate ? *c + x : x;
-                } else if (g.epi == kStoreT) {
-                    float* c = g.C + (int64_t)n * g.ldc + m;
-                    *c = g.accumulate ? *c + x : x;
+                if (g.epi == kStore || g.epi == kStoreT) {
+                    float* c = g.epi == kStore ? g.C + (int64_t)m * g.ldc + n : g.C + (int64_t)n * g.ldc + m;
+                    if (gridDim.z > 1) atomicAdd(c, x);
+                    else *c = g.accumulate ? *c + x : x;
                 } else {
                     if (g.epi == kGeluBack) {
                         float d;
@@ -178,11 +193,22 @@ __global__ void __launch_bounds__(128) mlp_gemm_tc_kernel(TcArgs g) {
 
 template <int NT>
 cudaError_t launch_tc(const TcArgs& a, cudaStream_t s) {
-    const size_t smem = 2 * (size_t)(kTM * kKC * 2 + NT * kKC * 2) + 64;
+    const size_t smem = kStages * (size_t)(kTM * kKC * 2 + NT * kKC * 2) + 64;
     cudaError_t e = cudaFuncSetAttribute(mlp_gemm_tc_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    dim3 grid((unsigned)(a.M / kTM), (unsigned)(a.N / NT));
+    // long reductions (the weight gradients, K = batch) are split over up to
+    // eight CTAs of at least two chunks each, which add their parts atomically
+    int split = 1;
+    if (a.epi == kStore || a.epi == kStoreT) split = std::max(1, std::min(8, a.K / (2 * kKC)));
+    if (split > 1 && !a.accumulate) {
+        // the parts add into zero
+        const size_t w = (size_t)(a.epi == kStore ? a.N : a.M) * sizeof(float);
+        const size_t h = (size_t)(a.epi == kStore ? a.M : a.N);
+        e = cudaMemset2DAsync(a.C, (size_t)a.ldc * sizeof(float), 0, w, h, s);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid((unsigned)(a.M / kTM), (unsigned)(a.N / NT), (unsigned)split);
     mlp_gemm_tc_kernel<NT><<<grid, 128, smem, s>>>(a);
     return cudaGetLastError();
 }
