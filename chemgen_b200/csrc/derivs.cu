@@ -617,10 +617,14 @@ __global__ void __launch_bounds__(32 * kJMaxWarps, 1)
             double rk = ak * ctot;
             for (int j = 0; j < ns; ++j) rk = fma(row[(1 + j) * kJTile], sC[j * kJTile + lane], rk);
             if (act) {
+                // streaming stores: J is never read back, so its lines go
+                // first when L2 needs room and the tile's rate-constant cache
+                // stays resident instead of being written back to DRAM
                 JT* Jr = J + (int64_t)k * ncol * ng + i;
-                Jr[0] = (JT)(row[0] - rk * pt.invT);
+                __stcs(Jr, (JT)(row[0] - rk * pt.invT));
                 for (int j = 0; j < ns; ++j)
-                    Jr[(int64_t)(1 + j) * ng] = (JT)(fma(ctot, row[(1 + j) * kJTile] + ak, -rk) * __ldg(m.inv_mw + j) * iS);
+                    __stcs(Jr + (int64_t)(1 + j) * ng,
+                           (JT)(fma(ctot, row[(1 + j) * kJTile] + ak, -rk) * __ldg(m.inv_mw + j) * iS));
             }
         }
         __syncthreads();                     // the tile's state stays until every row is done
