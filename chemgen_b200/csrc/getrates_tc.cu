@@ -393,8 +393,10 @@ __global__ void __launch_bounds__(kTile * NT, 1)
         TileCtx c;
         c.C = sC;
         c.G = sG;
-        c.T = act ? Tg[i] : 1000.0;
-        c.Pv = act ? P[i] : kPatm;
+        // inputs are read once: streaming loads, so that they do not push the
+        // Gibbs scratch and the stoichiometry image out of L2
+        c.T = act ? __ldcs(Tg + i) : 1000.0;
+        c.Pv = act ? __ldcs(P + i) : kPatm;
         c.lnT = cgm::cg_log(c.T);
         c.invT = 1.0 / c.T;
         c.lnT2 = c.lnT * kLog2eD;
@@ -405,7 +407,7 @@ __global__ void __launch_bounds__(kTile * NT, 1)
         // by the thread with sub = k % NT
         double part = 0.0;
         for (int k = sub; k < ns; k += NT) {
-            const double yk = (act ? Y[(int64_t)k * ng + i] : 1.0) * __ldg(m.inv_mw + k);
+            const double yk = (act ? __ldcs(Y + (int64_t)k * ng + i) : 1.0) * __ldg(m.inv_mw + k);
             sG[k * kTile + pt] = yk;
             part += yk;
         }
@@ -449,10 +451,20 @@ __global__ void __launch_bounds__(kTile * NT, 1)
             const uint4* src = reinterpret_cast<const uint4*>(nu + (int64_t)ch * npad * kChunk);
             uint4* dst = reinterpret_cast<uint4*>(sB + buf * npad * 32);
             for (int q = tid; q < npad * 2; q += kTile * NT) dst[q] = __ldg(src + q);
-            // q for the chunk's reactions -> A operands (hi, mid, lo)
+            // q for the chunk's reactions -> A operands (hi, mid, lo).  The
+            // thread with share `sub` takes kPer consecutive reactions, so that
+            // its BF16 values of a row leave in one 8- or 16-byte store per
+            // split instead of one 2-byte store per reaction
             unsigned char* a0 = sA + buf * 3 * kABytes;
-            for (int j = sub; j < kChunk; j += NT) {
-                const int r = ch * kChunk + j;
+            constexpr int kPer = kChunk / NT, kWords = kPer / 4;
+            static_assert(kChunk % NT == 0 && kPer % 4 == 0, "each share takes whole 4-reaction words");
+            const int j0 = sub * kPer;
+            uint64_t ph[kWords], pm[kWords], pl[kWords];
+#pragma unroll
+            for (int w = 0; w < kWords; ++w) ph[w] = pm[w] = pl[w] = 0ull;
+#pragma unroll 1
+            for (int u = 0; u < kPer; ++u) {
+                const int r = ch * kChunk + j0 + u;
                 float q = 0.0f;
                 if (r < m.nr) {
                     const TcFast F = load_fast(fast + r);
@@ -463,10 +475,21 @@ __global__ void __launch_bounds__(kTile * NT, 1)
                 const float r1 = q - __bfloat162float(h);
                 const __nv_bfloat16 md = __float2bfloat16_rn(r1);
                 const __nv_bfloat16 lo = __float2bfloat16_rn(r1 - __bfloat162float(md));
-                const uint32_t off = um::kmajor_offset(pt, j, kChunk);
-                *reinterpret_cast<__nv_bfloat16*>(a0 + off) = h;
-                *reinterpret_cast<__nv_bfloat16*>(a0 + kABytes + off) = md;
-                *reinterpret_cast<__nv_bfloat16*>(a0 + 2 * kABytes + off) = lo;
+                const int sh = 16 * (u & 3);
+#pragma unroll
+                for (int w = 0; w < kWords; ++w)
+                    if (w == (u >> 2)) {
+                        ph[w] |= (uint64_t)__bfloat16_as_ushort(h) << sh;
+                        pm[w] |= (uint64_t)__bfloat16_as_ushort(md) << sh;
+                        pl[w] |= (uint64_t)__bfloat16_as_ushort(lo) << sh;
+                    }
+            }
+#pragma unroll
+            for (int w = 0; w < kWords; ++w) {
+                const uint32_t off = um::kmajor_offset(pt, j0 + 4 * w, kChunk);   // 8-byte aligned
+                *reinterpret_cast<uint64_t*>(a0 + off) = ph[w];
+                *reinterpret_cast<uint64_t*>(a0 + kABytes + off) = pm[w];
+                *reinterpret_cast<uint64_t*>(a0 + 2 * kABytes + off) = pl[w];
             }
             um::fence_proxy_async();
             um::fence_before_sync();
@@ -548,7 +571,10 @@ __global__ void __launch_bounds__(kTile * NT, 1)
                                     double x = (double)v[j];
                                     if (h64) x += __hiloint2double((int)d[2 * j + 1], (int)d[2 * j]);
                                     double* w = wdot + (int64_t)sp * ng + i;
-                                    *w = first_group ? x : *w + x;
+                                    // first (often only) group: a streaming store, so that
+                                    // wdot does not push the Gibbs scratch out of L2
+                                    if (first_group) __stcs(w, x);
+                                    else *w += x;
                                 }
                             }
                     }

@@ -72,9 +72,6 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
                  : "memory");
 }
 
-__device__ __forceinline__ void cp_async_wait_all() {
-    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-}
 
 template <int NT>
 __global__ void __launch_bounds__(128) mlp_gemm_tc_kernel(TcArgs g) {
@@ -83,7 +80,8 @@ __global__ void __launch_bounds__(128) mlp_gemm_tc_kernel(TcArgs g) {
     constexpr int kBBytes = NT * kKC * 2;
     constexpr int kStage = kABytes + kBBytes;
     constexpr uint32_t kCols = NT < 32 ? 32u : (uint32_t)NT;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + kStages * kStage);
+    constexpr int kPipe = kStages * kStage, kEpi = 4 * 32 * ((NT + 4) * 4 + (NT + 8) * 2);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + (kPipe > kEpi ? kPipe : kEpi));
     uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + kStages);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * kTM, n0 = blockIdx.y * NT;
@@ -155,35 +153,107 @@ __global__ void __launch_bounds__(128) mlp_gemm_tc_kernel(TcArgs g) {
     um::fence_after_sync();
     const int m = m0 + 32 * warp + lane;
     if (ok && nit > 0) {
+        // Epilogue.  Thread `lane` of warp w holds accumulator row m0 + 32 w +
+        // lane; the row-major outputs (C, H) and the zprev input go through a
+        // per-warp shared-memory stage ([32][NT + 4] FP32 and [32][NT + 8]
+        // BF16, in the pipeline's buffers, now idle), so that global memory
+        // sees whole rows; the transposed outputs (C for STORE_T, HT) are
+        // stored straight from the thread, where lanes already run along m.
+        constexpr int kLd = NT + 4, kLh = NT + 8;
+        float* stg = reinterpret_cast<float*>(sm) + warp * 32 * kLd;
+        bf16* hst = reinterpret_cast<bf16*>(reinterpret_cast<float*>(sm) + 4 * 32 * kLd) + warp * 32 * kLh;
+        const int64_t mrow0 = m0 + 32 * warp;
+        const bool rowC = g.C && g.epi != kStoreT;
+        const bool rowH = g.H != nullptr;
+        if (g.epi == kGeluBack) {
+            for (int r = 0; r < 32; ++r)
+                for (int c = 4 * lane; c < NT; c += 128)
+                    *reinterpret_cast<float4*>(stg + r * kLd + c) =
+                        __ldg(reinterpret_cast<const float4*>(g.zprev + (mrow0 + r) * g.ldz + n0 + c));
+            __syncwarp();
+        }
 #pragma unroll 1
         for (int c0 = 0; c0 < NT; c0 += 16) {
             float v[16];
             um::tmem_ld16(um::tmem_lane_addr(tbase, warp, c0), v);
             const int nb = n0 + c0;
+            float* srow = stg + lane * kLd + c0;
+            if (g.epi == kStoreT) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int n = nb + j;
-                float x = v[j];
-                if (g.epi == kStore || g.epi == kStoreT) {
-                    float* c = g.epi == kStore ? g.C + (int64_t)m * g.ldc + n : g.C + (int64_t)n * g.ldc + m;
-                    if (gridDim.z > 1) atomicAdd(c, x);
-                    else *c = g.accumulate ? *c + x : x;
-                } else {
-                    if (g.epi == kGeluBack) {
-                        float d;
-                        gelu(g.zprev[(int64_t)m * g.ldz + n], &d);
-                        x *= d;
-                    } else {
-                        x += g.bias[n];
-                    }
-                    if (g.C) g.C[(int64_t)m * g.ldc + n] = x;
-                    const float h = g.epi == kBiasGelu ? gelu(x, nullptr) : x;
-                    const bf16 hb = __float2bfloat16(h);
-                    if (g.H) g.H[(int64_t)m * g.ldh + n] = hb;
-                    if (g.HT) g.HT[(int64_t)n * g.ldt + m] = hb;
+                for (int j = 0; j < 16; ++j) {
+                    float* c = g.C + (int64_t)(nb + j) * g.ldc + m;
+                    if (gridDim.z > 1) atomicAdd(c, v[j]);
+                    else *c = g.accumulate ? *c + v[j] : v[j];
                 }
+                continue;
             }
+            if (g.epi == kGeluBack) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float4 z = *reinterpret_cast<const float4*>(srow + 4 * q);
+                    float d;
+                    gelu(z.x, &d); v[4 * q] *= d;
+                    gelu(z.y, &d); v[4 * q + 1] *= d;
+                    gelu(z.z, &d); v[4 * q + 2] *= d;
+                    gelu(z.w, &d); v[4 * q + 3] *= d;
+                }
+            } else if (g.epi == kBias || g.epi == kBiasGelu) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] += __ldg(g.bias + nb + j);
+            }
+            if (rowC)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    *reinterpret_cast<float4*>(srow + 4 * q) = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            if (g.epi == kStore) continue;
+            uint32_t hb[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                float h0 = v[2 * j], h1 = v[2 * j + 1];
+                if (g.epi == kBiasGelu) {
+                    h0 = gelu(h0, nullptr);
+                    h1 = gelu(h1, nullptr);
+                }
+                const __nv_bfloat162 pr = __floats2bfloat162_rn(h0, h1);
+                hb[j] = *reinterpret_cast<const uint32_t*>(&pr);
+            }
+            if (rowH) {
+                uint4* hrow = reinterpret_cast<uint4*>(hst + lane * kLh + c0);
+                hrow[0] = make_uint4(hb[0], hb[1], hb[2], hb[3]);
+                hrow[1] = make_uint4(hb[4], hb[5], hb[6], hb[7]);
+            }
+            if (g.HT)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    g.HT[(int64_t)(nb + 2 * j) * g.ldt + m] = __ushort_as_bfloat16((unsigned short)(hb[j] & 0xffffu));
+                    g.HT[(int64_t)(nb + 2 * j + 1) * g.ldt + m] = __ushort_as_bfloat16((unsigned short)(hb[j] >> 16));
+                }
         }
+        __syncwarp();
+        // whole rows out: FP32 C (4 floats a lane), BF16 H (8 a lane)
+        if (rowC)
+            for (int r = 0; r < 32; ++r)
+                for (int c = 4 * lane; c < NT; c += 128) {
+                    const float4 x = *reinterpret_cast<const float4*>(stg + r * kLd + c);
+                    float* dst = g.C + (mrow0 + r) * g.ldc + n0 + c;
+                    if (gridDim.z > 1) {
+                        atomicAdd(dst, x.x);
+                        atomicAdd(dst + 1, x.y);
+                        atomicAdd(dst + 2, x.z);
+                        atomicAdd(dst + 3, x.w);
+                    } else if (g.accumulate) {
+                        float4 y = *reinterpret_cast<const float4*>(dst);
+                        y.x += x.x; y.y += x.y; y.z += x.z; y.w += x.w;
+                        *reinterpret_cast<float4*>(dst) = y;
+                    } else {
+                        *reinterpret_cast<float4*>(dst) = x;
+                    }
+                }
+        if (rowH)
+            for (int r = 0; r < 32; ++r)
+                for (int c = 8 * lane; c < NT; c += 256)
+                    *reinterpret_cast<uint4*>(g.H + (mrow0 + r) * g.ldh + n0 + c) =
+                        *reinterpret_cast<const uint4*>(hst + r * kLh + c);
     }
     if (!ok && lane == 0) atomicExch(&g_mlp_tc_err, 1);
     um::fence_before_sync();
@@ -193,7 +263,10 @@ __global__ void __launch_bounds__(128) mlp_gemm_tc_kernel(TcArgs g) {
 
 template <int NT>
 cudaError_t launch_tc(const TcArgs& a, cudaStream_t s) {
-    const size_t smem = kStages * (size_t)(kTM * kKC * 2 + NT * kKC * 2) + 64;
+    // the pipeline's stages, or the epilogue's per-warp stages if larger
+    const size_t pipe = kStages * (size_t)(kTM * kKC * 2 + NT * kKC * 2);
+    const size_t epi = 4 * 32 * ((size_t)(NT + 4) * 4 + (size_t)(NT + 8) * 2);
+    const size_t smem = std::max(pipe, epi) + 64;
     cudaError_t e = cudaFuncSetAttribute(mlp_gemm_tc_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
@@ -231,6 +304,10 @@ extern "C" int chemgen_mlp_gemm_tc(const void* A, int64_t lda, const void* B, in
     if (lda < K || ldb < K || (C && ldc < (epilogue == kStoreT ? M : N)) || (H && ldh < N) || (HT && ldt < M))
         return CHEMGEN_ERR_INVALID_ARGUMENT;
     if (!al16(A) || !al16(B) || (lda & 7) || (ldb & 7)) return CHEMGEN_ERR_MISALIGNED;
+    // the epilogue moves whole rows of C / zprev (4 floats) and H (8 BF16) at a time
+    if (C && epilogue != kStoreT && (!al16(C) || (ldc & 3))) return CHEMGEN_ERR_MISALIGNED;
+    if (epilogue == kGeluBack && (!al16(zprev) || (ldz & 3))) return CHEMGEN_ERR_MISALIGNED;
+    if (H && (!al16(H) || (ldh & 7))) return CHEMGEN_ERR_MISALIGNED;
     TcArgs a{(const bf16*)A, lda, (const bf16*)B, ldb, M, N, K, epilogue, bias, zprev, ldz,
              C, ldc, (bf16*)H, ldh, (bf16*)HT, ldt, accumulate};
     cudaStream_t s = (cudaStream_t)stream;
@@ -277,5 +354,372 @@ extern "C" int chemgen_mlp_transpose_bf16(const void* src, int64_t lds, int rows
     dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
     transpose_bf16_kernel<<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>((const bf16*)src, lds, (bf16*)dst, ldd, rows,
                                                                         cols);
+    return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA;
+}
+
+namespace {
+// One Adam step over all of the network's tensors in one launch, which also
+// writes the operands the tensor-core products read: the BF16 copy of a
+// weight matrix [rows x cols] (wb), its transpose [cols x rows] (wt) and the
+// first layer's doubled copy [rows x 2 cols] for its hi + lo inputs (wd).
+constexpr int kAdamMax = 8;
+struct AdamTensor {
+    float* w;
+    const float* g;
+    float* m;
+    float* v;
+    bf16* wb;
+    bf16* wt;
+    bf16* wd;
+    int rows, cols;
+    float decay;
+};
+struct AdamArgs {
+    AdamTensor t[kAdamMax];
+    int64_t off[kAdamMax + 1];
+    int count;
+    const float* hyper;
+    float b1, b2, eps;
+};
+
+__global__ void adam_multi_kernel(AdamArgs a) {
+    const float lr = a.hyper[0], c1 = a.hyper[1], c2 = a.hyper[2];
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < a.off[a.count];
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int k = 0;
+        while (k + 1 < a.count && e >= a.off[k + 1]) ++k;
+        const AdamTensor& t = a.t[k];
+        const int64_t i = e - a.off[k];
+        const float gi = t.g[i] + t.decay * t.w[i];
+        const float mi = a.b1 * t.m[i] + (1.0f - a.b1) * gi;
+        const float vi = a.b2 * t.v[i] + (1.0f - a.b2) * gi * gi;
+        t.m[i] = mi;
+        t.v[i] = vi;
+        const float wi = t.w[i] - lr * (mi * c1) / (sqrtf(vi * c2) + a.eps);
+        t.w[i] = wi;
+        const bf16 h = __float2bfloat16(wi);
+        if (t.wb) t.wb[i] = h;
+        const int r = (int)(i / t.cols), c = (int)(i % t.cols);
+        if (t.wt) t.wt[(int64_t)c * t.rows + r] = h;
+        if (t.wd) {
+            t.wd[(int64_t)r * 2 * t.cols + c] = h;
+            t.wd[(int64_t)r * 2 * t.cols + t.cols + c] = h;
+        }
+    }
+}
+}  // namespace
+
+extern "C" int chemgen_mlp_adam_multi(int count, float* const* w, const float* const* g, float* const* m,
+                                      float* const* v, void* const* wb, void* const* wt, void* const* wd,
+                                      const int* rows, const int* cols, const float* decay, const float* hyper,
+                                      float b1, float b2, float eps, void* stream) {
+    if (count < 1 || count > kAdamMax || !w || !g || !m || !v || !rows || !cols || !hyper)
+        return CHEMGEN_ERR_INVALID_ARGUMENT;
+    AdamArgs a{};
+    a.count = count;
+    a.hyper = hyper;
+    a.b1 = b1;
+    a.b2 = b2;
+    a.eps = eps;
+    a.off[0] = 0;
+    for (int k = 0; k < count; ++k) {
+        if (!w[k] || !g[k] || !m[k] || !v[k] || rows[k] < 1 || cols[k] < 1) return CHEMGEN_ERR_INVALID_ARGUMENT;
+        a.t[k] = AdamTensor{w[k], g[k], m[k], v[k], wb ? (bf16*)wb[k] : nullptr, wt ? (bf16*)wt[k] : nullptr,
+                            wd ? (bf16*)wd[k] : nullptr, rows[k], cols[k], decay ? decay[k] : 0.0f};
+        a.off[k + 1] = a.off[k] + (int64_t)rows[k] * cols[k];
+    }
+    const int64_t n = a.off[count];
+    const int blocks = (int)std::min<int64_t>((n + 255) / 256, 4096);
+    adam_multi_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(a);
+    return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA;
+}
+
+// ---------------------------------------------------------------------------
+// Fused training passes.  One CTA of 256 threads owns a tile of 128 batch
+// rows (tensor-memory lanes) and runs a whole chain of products on it, the
+// activations staying in shared memory between layers:
+//   forward : Z_l = H_{l-1} W_l^T + b_l, H_l = GELU(Z_l) for the three hidden
+//             layers (H_{-1} = the input), out = H_2 W_3^T + b_3;
+//   backward: dZ_2 = (dout W_3) * GELU'(Z_2), dZ_1 = (dZ_2 W_2) * GELU'(Z_1),
+//             dZ_0 = (dZ_1 W_1) * GELU'(Z_0), and the bias gradients
+//             (column sums of dZ_l over the batch).
+// Per layer one thread issues the K/16 MMAs (M = 128, N = 256 or 64, BF16,
+// FP32 accumulation in 256 tensor-memory columns) against the layer's B
+// operand, which all threads copy into shared memory (16-byte cp.async into
+// the canonical K-major layout) while the previous epilogue runs.  Warp w
+// reads lane quadrant w % 4 and column half w / 4 of the accumulator.  What
+// the weight-gradient products need leaves transposed, [feature][row], where
+// a warp's lanes write consecutive addresses: Z_l (FP32), H_l and dZ_l (BF16),
+// dout.  Shared memory: 64 KB activations, 32 KB input, 128 KB weights.
+namespace {
+constexpr int kFR = 128, kFT = 256, kFHid = 256, kFOut = 64;
+constexpr uint32_t kFAOff = 0, kFXOff = kFR * kFHid * 2, kFWOff = kFXOff + kFR * 128 * 2,
+                   kFTail = kFWOff + kFHid * kFHid * 2;
+constexpr size_t kFSmem = (size_t)kFTail + 64;
+
+// rows x K BF16 (row stride ld elements, K-major) -> canonical K-major tile
+__device__ __forceinline__ void fused_load(unsigned char* dst, const bf16* src, int64_t ld, int rows, int K) {
+    const int per = K / 8;
+    for (int c = threadIdx.x; c < rows * per; c += kFT) {
+        const int r = c / per, kk = (c - r * per) * 8;
+        cp_async16(dst + um::kmajor_offset(r, kk, K), src + (int64_t)r * ld + kk);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void fused_mma(uint32_t tbase, const unsigned char* a, const unsigned char* b, int K,
+                                          int N, uint64_t* bar) {
+    um::fence_after_sync();
+    const uint32_t idesc = um::idesc_bf16(kFR, N), sa = um::smem_addr(a), sb = um::smem_addr(b);
+    for (int ks = 0; ks < K / 16; ++ks)
+        um::mma_bf16(tbase, um::desc_kmajor(sa, K, ks), um::desc_kmajor(sb, K, ks), idesc, ks > 0 ? 1u : 0u);
+    um::commit(bar);
+}
+
+// copies landed and shared-memory writes visible to the tensor core; tensor
+// memory reads ordered before the next MMA
+__device__ __forceinline__ void fused_step_end() {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    um::fence_proxy_async();
+    um::fence_before_sync();
+    __syncthreads();
+}
+
+struct FwdArgs {
+    const bf16* X;
+    int64_t ldx;
+    int K0;
+    const bf16* W[4];
+    const float* b[4];
+    int B;
+    float* ZT[3];
+    bf16* HT[3];
+    float* out;
+};
+
+__global__ void __launch_bounds__(kFT, 1) mlp_forward_fused_kernel(FwdArgs a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    unsigned char* sA = sm + kFAOff;
+    unsigned char* sX = sm + kFXOff;
+    unsigned char* sW = sm + kFWOff;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kFTail);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g4 = warp & 3, half = warp >> 2, row = 32 * g4 + lane;
+    const int64_t m0 = (int64_t)blockIdx.x * kFR, m = m0 + row;
+    if (tid == 0) {
+        um::mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) um::tmem_alloc(tslot, 256);
+    fused_load(sX, a.X + m0 * a.ldx, a.ldx, kFR, a.K0);
+    fused_load(sW, a.W[0], a.K0, kFHid, a.K0);
+    fused_step_end();
+    um::fence_after_sync();
+    const uint32_t tbase = *tslot;
+    uint32_t parity = 0;
+    bool ok = true;
+    for (int l = 0; l < 4 && ok; ++l) {
+        const int K = l == 0 ? a.K0 : kFHid, N = l == 3 ? kFOut : kFHid;
+        if (tid == 0) fused_mma(tbase, l == 0 ? sX : sA, sW, K, N, bar);
+        ok = um::mbar_wait(bar, parity);
+        parity ^= 1u;
+        um::fence_after_sync();
+        if (!ok) break;
+        // the next layer's weights stream in while this epilogue runs
+        if (l < 3) fused_load(sW, a.W[l + 1], kFHid, l == 2 ? kFOut : kFHid, kFHid);
+        if (l < 3) {
+            const float* bl = a.b[l];
+#pragma unroll 1
+            for (int c = 128 * half; c < 128 * half + 128; c += 16) {
+                float v[16];
+                um::tmem_ld16(um::tmem_lane_addr(tbase, g4, c), v);
+                uint32_t pk[8];
+#pragma unroll
+                for (int j = 0; j < 16; j += 2) {
+                    const float z0 = v[j] + __ldg(bl + c + j), z1 = v[j + 1] + __ldg(bl + c + j + 1);
+                    a.ZT[l][(int64_t)(c + j) * a.B + m] = z0;
+                    a.ZT[l][(int64_t)(c + j + 1) * a.B + m] = z1;
+                    const __nv_bfloat162 h = __floats2bfloat162_rn(gelu(z0, nullptr), gelu(z1, nullptr));
+                    a.HT[l][(int64_t)(c + j) * a.B + m] = h.x;
+                    a.HT[l][(int64_t)(c + j + 1) * a.B + m] = h.y;
+                    pk[j / 2] = *reinterpret_cast<const uint32_t*>(&h);
+                }
+                *reinterpret_cast<uint4*>(sA + um::kmajor_offset(row, c, kFHid)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                *reinterpret_cast<uint4*>(sA + um::kmajor_offset(row, c + 8, kFHid)) =
+                    make_uint4(pk[4], pk[5], pk[6], pk[7]);
+            }
+        } else {
+#pragma unroll 1
+            for (int c = 32 * half; c < 32 * half + 32; c += 16) {
+                float v[16];
+                um::tmem_ld16(um::tmem_lane_addr(tbase, g4, c), v);
+                float4* o = reinterpret_cast<float4*>(a.out + m * kFOut + c);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    o[q] = make_float4(v[4 * q] + __ldg(a.b[3] + c + 4 * q), v[4 * q + 1] + __ldg(a.b[3] + c + 4 * q + 1),
+                                       v[4 * q + 2] + __ldg(a.b[3] + c + 4 * q + 2),
+                                       v[4 * q + 3] + __ldg(a.b[3] + c + 4 * q + 3));
+            }
+        }
+        fused_step_end();
+    }
+    if (!ok && lane == 0) atomicExch(&g_mlp_tc_err, 1);
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    um::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) um::tmem_dealloc(tbase, 256);
+}
+
+struct BwdArgs {
+    const bf16* dout;      // [B x 64]
+    const bf16* WT[4];     // W_l^T [in x out]; 1..3 used
+    const float* ZT[3];
+    int B;
+    bf16* dZT[3];
+    float* gb[3];          // accumulated (atomically) column sums
+    bf16* doutT;           // [64 x B]
+};
+
+__global__ void __launch_bounds__(kFT, 1) mlp_backward_fused_kernel(BwdArgs a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    unsigned char* sA = sm + kFAOff;
+    unsigned char* sX = sm + kFXOff;
+    unsigned char* sW = sm + kFWOff;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kFTail);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g4 = warp & 3, half = warp >> 2, row = 32 * g4 + lane;
+    const int64_t m0 = (int64_t)blockIdx.x * kFR, m = m0 + row;
+    if (tid == 0) {
+        um::mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) um::tmem_alloc(tslot, 256);
+    fused_load(sX, a.dout + m0 * kFOut, kFOut, kFR, kFOut);
+    fused_load(sW, a.WT[3], kFOut, kFHid, kFOut);
+    fused_step_end();
+    um::fence_after_sync();
+    const uint32_t tbase = *tslot;
+    // dout transposed for the last layer's weight gradient, from the tile copy
+    for (int n = 32 * half; n < 32 * half + 32; ++n)
+        a.doutT[(int64_t)n * a.B + m] = *reinterpret_cast<const bf16*>(sX + um::kmajor_offset(row, n, kFOut));
+    uint32_t parity = 0;
+    bool ok = true;
+    for (int s = 0; s < 3 && ok; ++s) {
+        const int L = 3 - s, K = s == 0 ? kFOut : kFHid;     // weight layer, its output width
+        if (tid == 0) fused_mma(tbase, s == 0 ? sX : sA, sW, K, kFHid, bar);
+        ok = um::mbar_wait(bar, parity);
+        parity ^= 1u;
+        um::fence_after_sync();
+        if (!ok) break;
+        if (s < 2) fused_load(sW, a.WT[L - 1], kFHid, kFHid, kFHid);
+        const float* z = a.ZT[L - 1];
+        bf16* dzt = a.dZT[L - 1];
+        float* gb = a.gb[L - 1];
+#pragma unroll 1
+        for (int c = 128 * half; c < 128 * half + 128; c += 16) {
+            float v[16];
+            um::tmem_ld16(um::tmem_lane_addr(tbase, g4, c), v);
+            uint32_t pk[8];
+#pragma unroll
+            for (int j = 0; j < 16; j += 2) {
+                float d0, d1;
+                gelu(z[(int64_t)(c + j) * a.B + m], &d0);
+                gelu(z[(int64_t)(c + j + 1) * a.B + m], &d1);
+                v[j] *= d0;
+                v[j + 1] *= d1;
+                const __nv_bfloat162 h = __floats2bfloat162_rn(v[j], v[j + 1]);
+                dzt[(int64_t)(c + j) * a.B + m] = h.x;
+                dzt[(int64_t)(c + j + 1) * a.B + m] = h.y;
+                pk[j / 2] = *reinterpret_cast<const uint32_t*>(&h);
+            }
+            if (s < 2) {
+                *reinterpret_cast<uint4*>(sA + um::kmajor_offset(row, c, kFHid)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                *reinterpret_cast<uint4*>(sA + um::kmajor_offset(row, c + 8, kFHid)) =
+                    make_uint4(pk[4], pk[5], pk[6], pk[7]);
+            }
+            // bias gradient: the column sums of this warp's 32 rows (FP32)
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                float t = v[j];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+                if (lane == 0) atomicAdd(gb + c + j, t);
+            }
+        }
+        fused_step_end();
+    }
+    if (!ok && lane == 0) atomicExch(&g_mlp_tc_err, 1);
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    um::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) um::tmem_dealloc(tbase, 256);
+}
+
+bool fused_ready() {
+    static int st = -1;
+    if (st < 0) {
+        st = cudaFuncSetAttribute(mlp_forward_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kFSmem) == cudaSuccess &&
+                     cudaFuncSetAttribute(mlp_backward_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)kFSmem) == cudaSuccess
+                 ? 1
+                 : 0;
+    }
+    return st == 1;
+}
+}  // namespace
+
+extern "C" int chemgen_mlp_forward_tc(const void* X, int64_t ldx, int K0, const void* const* W, const float* const* b,
+                                      int B, float* const* ZT, void* const* HT, float* out, void* stream) {
+    if (!X || !W || !b || !ZT || !HT || !out || B <= 0 || B % kFR || (K0 != 64 && K0 != 128) || ldx < K0)
+        return CHEMGEN_ERR_INVALID_ARGUMENT;
+    FwdArgs a{};
+    a.X = (const bf16*)X;
+    a.ldx = ldx;
+    a.K0 = K0;
+    a.B = B;
+    a.out = out;
+    for (int l = 0; l < 4; ++l) {
+        if (!W[l] || !b[l] || !al16(W[l])) return W[l] && b[l] ? CHEMGEN_ERR_MISALIGNED : CHEMGEN_ERR_INVALID_ARGUMENT;
+        a.W[l] = (const bf16*)W[l];
+        a.b[l] = b[l];
+    }
+    for (int l = 0; l < 3; ++l) {
+        if (!ZT[l] || !HT[l]) return CHEMGEN_ERR_INVALID_ARGUMENT;
+        a.ZT[l] = ZT[l];
+        a.HT[l] = (bf16*)HT[l];
+    }
+    if (!al16(X) || (ldx & 7) || !al16(out)) return CHEMGEN_ERR_MISALIGNED;
+    if (!fused_ready()) return CHEMGEN_ERR_CUDA;
+    mlp_forward_fused_kernel<<<B / kFR, kFT, kFSmem, (cudaStream_t)stream>>>(a);
+    return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA;
+}
+
+extern "C" int chemgen_mlp_backward_tc(const void* dout, const void* const* WT, const float* const* ZT, int B,
+                                       void* const* dZT, float* const* gb, void* doutT, void* stream) {
+    if (!dout || !WT || !ZT || !dZT || !gb || !doutT || B <= 0 || B % kFR) return CHEMGEN_ERR_INVALID_ARGUMENT;
+    BwdArgs a{};
+    a.dout = (const bf16*)dout;
+    a.B = B;
+    a.doutT = (bf16*)doutT;
+    for (int l = 1; l < 4; ++l) {
+        if (!WT[l]) return CHEMGEN_ERR_INVALID_ARGUMENT;
+        if (!al16(WT[l])) return CHEMGEN_ERR_MISALIGNED;
+        a.WT[l] = (const bf16*)WT[l];
+    }
+    for (int l = 0; l < 3; ++l) {
+        if (!ZT[l] || !dZT[l] || !gb[l]) return CHEMGEN_ERR_INVALID_ARGUMENT;
+        a.ZT[l] = ZT[l];
+        a.dZT[l] = (bf16*)dZT[l];
+        a.gb[l] = gb[l];
+    }
+    if (!al16(dout)) return CHEMGEN_ERR_MISALIGNED;
+    if (!fused_ready()) return CHEMGEN_ERR_CUDA;
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int l = 0; l < 3; ++l)
+        if (cudaMemsetAsync(gb[l], 0, kFHid * sizeof(float), s) != cudaSuccess) return CHEMGEN_ERR_CUDA;
+    mlp_backward_fused_kernel<<<B / kFR, kFT, kFSmem, s>>>(a);
     return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA;
 }

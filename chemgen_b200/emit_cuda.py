@@ -32,7 +32,11 @@ LOG10_2 = 0.30102999566398119521
 CSCALE_LOG2 = 32          # mixed: concentrations are stored as C * 2^32 in FP32
 # register-resident wdot accumulators up to this many species
 MAX_REG_SPECIES = 72
-SYNC_EVERY = 48           # reactions between block barriers, FP64 kernel (B200 sweep at 53/325: 2..64)
+SYNC_EVERY = 96           # reactions between block barriers, FP64 kernel (B200 sweeps at 53/325: 2..128, 0)
+# FP64 kernel: consecutive reactions whose tensor-memory values load behind one wait
+# (B200 at 53/325, 2^20 points: 1 -> 509-530, 3 -> 541-554 Mpts/s with barriers every 64-96
+# reactions or none; 2, 4 and 6 gained less)
+EGP_GROUP = 3
 SYNC_EVERY_MIXED = 24     # mixed kernel (B200 sweep at 53/325: 16..96, best 24-48)
 SMEM_BUDGET = 220 * 1024  # dynamic shared memory per block
 REG_FILE = 65536          # 32-bit registers per SM
@@ -119,8 +123,13 @@ def _f(x: float) -> str:
 
 class _Emitter:
     def __init__(self, mech: Mechanism, block: int, sync_every: int = SYNC_EVERY, tmem: bool = False,
-                 live_order: bool = True, exp_noinline: bool = False, tm_prefetch: bool = False):
+                 live_order: bool = True, exp_noinline: bool = False, tm_prefetch: bool = False,
+                 egp_group: int = 1):
         self.sync_every = sync_every
+        # FP64 tensor-memory mode: the values of egp_group consecutive
+        # reactions load behind one wait, so that their arithmetic can overlap
+        self.egp_group = egp_group if (tmem and not tm_prefetch) else 1
+        self._egp_ready = False
         # reactions call out-of-line copies of the FP64 exp (shorter code)
         self.exp_noinline = exp_noinline
         # tensor-memory mode: a reversible reaction's values are loaded while
@@ -179,6 +188,23 @@ class _Emitter:
         self._eloc = {sp: f"e{j}_{n}" for n, sp in enumerate(sps)}
         L = [f"cgg::tm_wait_{len(sps)}(tq{j});"]
         L.append("const double " + ", ".join(f"e{j}_{n} = __hiloint2double((int)tq{j}[{2 * n + 1}], (int)tq{j}[{2 * n}])"
+                                             for n in range(len(sps))) + ";")
+        return L
+
+    def group_egp(self, p: int, rs: List[Reaction]) -> List[str]:
+        """Grouped mode: issue the loads of the EGp values the reversible
+        reactions in `rs` need, wait once, and name them for the reactions."""
+        sps = list(dict.fromkeys(sp for r in rs if r.reversible for sp in self._egp_species(r)))
+        self._egp_ready = True
+        self._eloc = {sp: f"g{p}_{n}" for n, sp in enumerate(sps)}
+        if not sps:
+            return []
+        L = [f"uint32_t gq{p}[{2 * len(sps)}];"]
+        for n, sp in enumerate(sps):
+            L.append(f"cgg::tm_issue(tw + {2 * self.idx[sp]}u, gq{p}[{2 * n}], gq{p}[{2 * n + 1}]);")
+        ops = ", ".join(f'"+r"(gq{p}[{k}])' for k in range(2 * len(sps)))
+        L.append(f'__syncwarp(); asm volatile("tcgen05.wait::ld.sync.aligned;" : {ops} :: "memory");')
+        L.append("const double " + ", ".join(f"g{p}_{n} = __hiloint2double((int)gq{p}[{2 * n + 1}], (int)gq{p}[{2 * n}])"
                                              for n in range(len(sps))) + ";")
         return L
 
@@ -352,7 +378,7 @@ class _Emitter:
             body += self.falloff64(r)
         qf = f"kf*{self.prod(r.reactants, self.C)}"
         if r.reversible:
-            if self.tmem and not self.tm_prefetch:
+            if self.tmem and not self.tm_prefetch and not self._egp_ready:
                 body += self.load_egp(r)
             num = self.prod(r.reactants, self.E)
             den = self.prod(r.products, self.E)
@@ -635,6 +661,9 @@ class _Emitter:
                 if new:
                     L.append("  double " + ", ".join(f"w{k} = 0.0" for k in new) + ";")
                     declared.update(new)
+            if not mixed and self.egp_group > 1 and p % self.egp_group == 0:
+                L += ["  " + x for x in self.group_egp(p, [self.mech.reactions[jj]
+                                                            for jj in order[p:p + self.egp_group]])]
             if rev_pos and r.reversible:
                 L += ["  " + x for x in self.wait_egp(j, r)]
                 if p in next_rev:
@@ -711,7 +740,7 @@ PRECISIONS = {"fp64": (True, False), "mixed": (False, True), "both": (True, True
 def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = None,
          sync_every: Optional[int] = None, precision: str = "both", tmem: Optional[bool] = None,
          live_order: bool = True, exp_noinline: bool = False, live_order_mixed: Optional[bool] = False,
-         tm_prefetch: bool = False) -> str:
+         tm_prefetch: bool = False, egp_group: Optional[int] = None) -> str:
     """CUDA source of the mechanism's kernels: `precision` selects the FP64
     kernel, the mixed one or both; a mode without a generated kernel runs on
     the table-driven kernels."""
@@ -724,7 +753,8 @@ def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = Non
     tm32 = use_tmem(mech.ns, True) if tmem is None else tmem
     em64 = _Emitter(mech, block or choose_block(mech.ns, False, tm64),
                     SYNC_EVERY if sync_every is None else sync_every, tmem=tm64, live_order=live_order,
-                    exp_noinline=exp_noinline, tm_prefetch=tm_prefetch)
+                    exp_noinline=exp_noinline, tm_prefetch=tm_prefetch,
+                    egp_group=EGP_GROUP if egp_group is None else egp_group)
     # the mixed kernel keeps file order unless asked: on B200 at 53/325 the live-range order made
     # the FP64 kernel 5 % faster (497 -> 522 Mpts/s) and the mixed one 2 % slower (794 -> 777)
     em32 = _Emitter(mech, block or choose_block(mech.ns, True, tm32),

@@ -87,11 +87,15 @@ def lib() -> ctypes.CDLL:
                                       ci, vp]
     L.chemgen_mlp_tc_error.argtypes = [ci]
     L.chemgen_mlp_transpose_bf16.argtypes = [vp, i64, ci, ci, vp, i64, vp]
+    L.chemgen_mlp_adam_multi.argtypes = [ci, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, f32, f32, f32, vp]
+    L.chemgen_mlp_forward_tc.argtypes = [vp, i64, ci, vp, vp, ci, vp, vp, vp, vp]
+    L.chemgen_mlp_backward_tc.argtypes = [vp, vp, vp, ci, vp, vp, vp, vp]
     L.chemgen_surrogate_image_elems.argtypes = []
     L.chemgen_surrogate_pack.argtypes = [vp, vp, vp, vp, vp, vp]
     L.chemgen_surrogate_infer.argtypes = [vp, vp, vp, vp, vp, ci, vp, vp, i64, vp, vp, vp, vp, vp]
     L.chemgen_surrogate_infer_error.argtypes = [ci]
     for f in ("chemgen_mlp_gemm", "chemgen_mlp_gemm_tc", "chemgen_mlp_tc_error", "chemgen_mlp_transpose_bf16",
+              "chemgen_mlp_adam_multi", "chemgen_mlp_forward_tc", "chemgen_mlp_backward_tc",
               "chemgen_mlp_bias_gelu", "chemgen_mlp_gelu_backward", "chemgen_mlp_mse_grad",
               "chemgen_mlp_colsum", "chemgen_mlp_adam", "chemgen_surrogate_features", "chemgen_surrogate_targets",
               "chemgen_surrogate_decode", "chemgen_surrogate_image_elems", "chemgen_surrogate_pack",

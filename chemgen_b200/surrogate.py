@@ -28,6 +28,7 @@ prototype (log-space Arrhenius layers) never ran.
 """
 from __future__ import annotations
 
+import ctypes
 import math
 import time
 from dataclasses import dataclass
@@ -54,6 +55,10 @@ class TrainConfig:
     lr_final: float = 5e-5
     weight_decay: float = 0.0
     error_head_epochs: int = 1
+    # the error head's target: 0 -> the mean of log10 normwise error (least
+    # squares); q in (0, 1) -> its q-quantile (pinball loss), a conservative
+    # estimate for the gate
+    error_quantile: float = 0.0
     seed: int = 0
 
 
@@ -117,14 +122,21 @@ class MLP:
         self.refresh_operands()
 
     def refresh_operands(self):
-        """Rebuild Wd0 and the transposed weights from the BF16 weights (after
-        every optimizer step; part of the captured training step)."""
+        """Rebuild Wd0 and the transposed weights from the BF16 weights (at
+        construction and after weights are loaded or changed outside the
+        training step, whose Adam launch writes them itself)."""
         for l in range(4):
             k, n = self.dims[l], self.dims[l + 1]
             _transpose(self.Wb[l], n, k, self.WT[l])
         din, hid = self.dims[0], self.dims[1]
         _transpose(self.WT[0], din, hid, self.Wd0, ldd=2 * din)
         _transpose(self.WT[0], din, hid, self.Wd0.data_ptr() + 2 * din, ldd=2 * din)
+
+    def _side_stream(self):
+        import torch
+        if getattr(self, "_side", None) is None:
+            self._side = torch.cuda.Stream(device=self.dev)
+        return self._side
 
     def _use_tc(self, B: int) -> bool:
         return self.tc and B % 128 == 0
@@ -158,6 +170,23 @@ class MLP:
         else:
             raise ValueError(f"input width {X.shape[1]} is neither {din} nor {2 * din}")
         self.acts, self.zs, self.actsT = [X], [], []
+        if keep:
+            # training: one fused kernel for the four layers; Z_l (FP32) and
+            # H_l (BF16) leave transposed, [feature][row], for the backward
+            ZT = [self._buf(("ZT", l), (hid, B), torch.float32) for l in range(3)]
+            HT = [self._buf(("HT", l), (hid, B), torch.bfloat16) for l in range(3)]
+            out = self._buf(("Z", 3, keep), (B, dout), torch.float32)
+            P = ctypes.c_void_p
+            Ws = (P * 4)(W0.data_ptr(), *[self.Wb[l].data_ptr() for l in (1, 2, 3)])
+            bs = (P * 4)(*[self.b[l].data_ptr() for l in range(4)])
+            check(lib().chemgen_mlp_forward_tc(X.data_ptr(), X.shape[1], K0, Ws, bs, B,
+                                               (P * 3)(*[z.data_ptr() for z in ZT]),
+                                               (P * 3)(*[h.data_ptr() for h in HT]), out.data_ptr(), _stream()),
+                  "mlp_forward_tc")
+            self.zs, self.actsT = ZT, HT
+            self.zs_transposed = True
+            return out
+        self.zs_transposed = False
         A, lda, Bw, K = X, X.shape[1], W0, K0
         for l in range(3):
             Z = self._buf(("Z", l, keep), (B, hid), torch.float32) if keep else None
@@ -175,38 +204,54 @@ class MLP:
         return out
 
     def _backward_tc(self, dout_b, dout_f):
+        """One fused kernel takes the input gradients dZ_2, dZ_1, dZ_0 down the
+        network (with the bias gradients and the transposed operands); the
+        weight-gradient products then run on two streams side by side (each
+        fills only 8-32 of the SMs), while a side stream has transposed the
+        input and summed the output gradient meanwhile.  The current stream
+        joins the side stream at the end (CUDA-graph capture keeps the fork
+        and join)."""
         import torch
         B = dout_b.shape[0]
-        s = _stream()
+        main = torch.cuda.current_stream()
+        side = self._side_stream()
         din, hid, dout = self.dims[0], self.dims[1], self.dims[4]
         gW = [self._buf(("gW", l), (self.dims[l + 1], self.dims[l]), torch.float32) for l in range(4)]
         gb = [self._buf(("gb", l), (self.dims[l + 1],), torch.float32) for l in range(4)]
         doutT = self._buf(("doutT",), (dout, B), torch.bfloat16)
-        _transpose(dout_b, B, dout, doutT)
-        # layer 3: dW3[n][k] = sum_m dout[m][n] H2[m][k], as (H2^T)(dout^T)^T stored transposed
-        _gemm_tc(self.actsT[2], B, doutT, B, hid, dout, B, EPI_STORE_T, C=gW[3], ldc=hid)
-        check(lib().chemgen_mlp_colsum(dout_f.data_ptr(), gb[3].data_ptr(), B, dout, s), "mlp_colsum")
-        dZb, dZf, dZT, n = dout_b, dout_f, doutT, dout
-        for l in range(2, -1, -1):
-            # dZ_l = (dZ_{l+1} W_{l+1}) * GELU'(Z_l)
-            nb = self._buf(("dZb", l), (B, hid), torch.bfloat16)
-            nf = self._buf(("dZf", l), (B, hid), torch.float32)
-            nT = self._buf(("dZT", l), (hid, B), torch.bfloat16)
-            _gemm_tc(dZb, n, self.WT[l + 1], n, B, hid, n, EPI_GELU_BACK, zprev=self.zs[l], ldz=hid, C=nf, ldc=hid,
-                     H=nb, ldh=hid, HT=nT, ldt=B)
-            dZb, dZf, dZT, n = nb, nf, nT, hid
-            check(lib().chemgen_mlp_colsum(dZf.data_ptr(), gb[l].data_ptr(), B, hid, s), "mlp_colsum")
-            if l > 0:
-                # dW_l[n][k] = sum_m dZ_l[m][n] H_{l-1}[m][k]
-                _gemm_tc(dZT, B, self.actsT[l - 1], B, hid, hid, B, EPI_STORE, C=gW[l], ldc=hid)
-        # layer 0: the input's transposed parts (hi, lo) as operands, summed
+        dZT = [self._buf(("dZT", l), (hid, B), torch.bfloat16) for l in range(3)]
         X = self.acts[0]
         w = X.shape[1]
         XT = self._buf(("XT",), (w, B), torch.bfloat16)
-        _transpose(X, B, w, XT)
-        for j in range(w // din):
-            _gemm_tc(dZT, B, XT.data_ptr() + 2 * j * din * B, B, hid, din, B, EPI_STORE, C=gW[0], ldc=din,
-                     accumulate=1 if j else 0)
+
+        def fork():
+            ev = torch.cuda.Event()
+            ev.record(main)
+            side.wait_event(ev)
+
+        fork()
+        with torch.cuda.stream(side):
+            check(lib().chemgen_mlp_colsum(dout_f.data_ptr(), gb[3].data_ptr(), B, dout, _stream()), "mlp_colsum")
+            _transpose(X, B, w, XT)
+        P = ctypes.c_void_p
+        check(lib().chemgen_mlp_backward_tc(dout_b.data_ptr(), (P * 4)(None, *[self.WT[l].data_ptr() for l in (1, 2, 3)]),
+                                            (P * 3)(*[z.data_ptr() for z in self.zs]), B,
+                                            (P * 3)(*[d.data_ptr() for d in dZT]),
+                                            (P * 3)(*[g.data_ptr() for g in gb[:3]]), doutT.data_ptr(), _stream()),
+              "mlp_backward_tc")
+        fork()
+        with torch.cuda.stream(side):
+            # dW3[n][k] = sum_m dout[m][n] H2[m][k], as (H2^T)(dout^T)^T stored transposed
+            _gemm_tc(self.actsT[2], B, doutT, B, hid, dout, B, EPI_STORE_T, C=gW[3], ldc=hid)
+            # layer 0: the input's transposed parts (hi, lo, transposed above on
+            # this stream) as operands, summed
+            for j in range(w // din):
+                _gemm_tc(dZT[0], B, XT.data_ptr() + 2 * j * din * B, B, hid, din, B, EPI_STORE, C=gW[0],
+                         ldc=din, accumulate=1 if j else 0)
+        # dW_l[n][k] = sum_m dZ_l[m][n] H_{l-1}[m][k]
+        _gemm_tc(dZT[2], B, self.actsT[1], B, hid, hid, B, EPI_STORE, C=gW[2], ldc=hid)
+        _gemm_tc(dZT[1], B, self.actsT[0], B, hid, hid, B, EPI_STORE, C=gW[1], ldc=hid)
+        main.wait_stream(side)
         return gW + gb
 
     def forward(self, X, keep: bool = True):
@@ -274,16 +319,42 @@ class MLP:
             dZb, dZf = nb, nf
         return gW + gb
 
+    def _adam_tables(self, grads, wd: float):
+        """Host pointer tables of chemgen_mlp_adam_multi for these gradient
+        buffers (cached: the buffers do not move between steps)."""
+        import ctypes
+        key = (tuple(g.data_ptr() for g in grads), wd)
+        if getattr(self, "_adam_key", None) != key:
+            n = len(self.params)
+            P = ctypes.c_void_p * n
+            rows = [p.shape[0] for p in self.params]
+            cols = [p.shape[1] if p.dim() == 2 else 1 for p in self.params]
+            self._adam_tab = (
+                P(*[p.data_ptr() for p in self.params]), P(*[g.data_ptr() for g in grads]),
+                P(*[m.data_ptr() for m in self.m]), P(*[v.data_ptr() for v in self.v]),
+                P(*[self.Wb[j].data_ptr() if j < 4 else None for j in range(n)]),
+                P(*[self.WT[j].data_ptr() if j < 4 else None for j in range(n)]),
+                P(*[self.Wd0.data_ptr() if j == 0 else None for j in range(n)]),
+                (ctypes.c_int * n)(*rows), (ctypes.c_int * n)(*cols),
+                (ctypes.c_float * n)(*[wd if j < 4 else 0.0 for j in range(n)]))
+            self._adam_key = key
+        return self._adam_tab
+
     def adam(self, grads, hyper, wd: float = 0.0, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8):
-        """One Adam step; `hyper` is a device FP32 tensor {lr, 1/(1-b1^t), 1/(1-b2^t)}."""
+        """One Adam step; `hyper` is a device FP32 tensor {lr, 1/(1-b1^t), 1/(1-b2^t)}.
+        With the tensor-core products, one launch updates every tensor and
+        writes the BF16, transposed and doubled operands."""
         s = _stream()
+        if self.tc:
+            t = self._adam_tables(grads, wd)
+            check(lib().chemgen_mlp_adam_multi(len(self.params), *t, hyper.data_ptr(), b1, b2, eps, s),
+                  "mlp_adam_multi")
+            return
         for j, (p, g) in enumerate(zip(self.params, grads)):
             wb = self.Wb[j].data_ptr() if j < 4 else 0
             check(lib().chemgen_mlp_adam(p.data_ptr(), g.data_ptr(), self.m[j].data_ptr(), self.v[j].data_ptr(), wb,
                                          p.numel(), hyper.data_ptr(), b1, b2, eps, wd if j < 4 else 0.0, s),
                   "mlp_adam")
-        if self.tc:
-            self.refresh_operands()
 
 
 def adam_schedule(total: int, lr: float, lr_final: float, b1: float = 0.9, b2: float = 0.999, device=None):
@@ -504,8 +575,18 @@ class Surrogate:
             tb = Tg.index_select(0, idx)
             out = self.net.forward(xb)
             tb[:, self.ns + 1] = self._normwise_error(out, tb)
-            check(lib().chemgen_mlp_mse_grad(out.data_ptr(), tb.data_ptr(), colw.data_ptr(), dout_b.data_ptr(),
-                                             dout_f.data_ptr(), loss.data_ptr(), xb.shape[0], DOUT, s), "mse_grad")
+            if cfg.error_quantile > 0.0:
+                # pinball loss: slope -q above the estimate, 1 - q below it
+                y, o = tb[:, self.ns + 1], out[:, self.ns + 1].float()
+                g = torch.where(y > o, -cfg.error_quantile, 1.0 - cfg.error_quantile) / xb.shape[0]
+                dout_f.zero_()
+                dout_f[: xb.shape[0], self.ns + 1] = g
+                dout_b.copy_(dout_f)
+                loss += (torch.maximum(cfg.error_quantile * (y - o), (cfg.error_quantile - 1.0) * (y - o))).mean()
+            else:
+                check(lib().chemgen_mlp_mse_grad(out.data_ptr(), tb.data_ptr(), colw.data_ptr(), dout_b.data_ptr(),
+                                                 dout_f.data_ptr(), loss.data_ptr(), xb.shape[0], DOUT, s),
+                      "mse_grad")
             grads = self.net.backward(dout_b[: xb.shape[0]], dout_f[: xb.shape[0]])
             # only the error-estimate output (row ns + 1 of the last layer and
             # its bias) moves, with its own Adam state
@@ -625,19 +706,27 @@ class Surrogate:
 
 
 class SurrogateGetrates:
-    """wdot from the surrogate where it is trusted, from the exact kernel elsewhere."""
+    """wdot from the surrogate where it is trusted, from the exact kernel elsewhere.
 
-    def __init__(self, sur: Surrogate, tol: float, exact_mode: str = "mixed"):
+    A point is trusted when its log10 error estimate is at most log10(tol) -
+    margin.  The estimate is a regression on the network's own features and
+    under-estimates some states at the edges of the training distribution;
+    a margin of 0.5 (a factor 3.2 on the estimate) trades more fallback for
+    a bounded worst case (on B200 at 53/325 with the default training:
+    fallback 0.15 % -> 6-29 %, max normwise error after fallback 15 -> ~1)."""
+
+    def __init__(self, sur: Surrogate, tol: float, exact_mode: str = "mixed", margin: float = 0.0):
         self.sur = sur
         self.tol = tol
         self.exact_mode = exact_mode
+        self.margin = margin
         self.last_fallback = 0.0
 
     def __call__(self, P, T, Y):
         import torch
         # the fused kernel folds the training-support check into the estimate
         W, est = self.sur.predict(P, T, Y, check_range=True)
-        ok = est <= math.log10(self.tol)
+        ok = est <= math.log10(self.tol) - self.margin
         bad = torch.nonzero(~ok).flatten()
         if bad.numel():
             Pb, Tb = P.index_select(0, bad).contiguous(), T.index_select(0, bad).contiguous()

@@ -177,16 +177,41 @@ int chemgen_surrogate_decode(const float* out, int64_t ng, int ns, int dout, con
  *   2 BIAS_GELU      z = acc + bias[n]; C = z (if C); H[m*ldh + n] and HT[n*ldt + m] = GELU(z) (BF16, if given)
  *   3 BIAS           z = acc + bias[n]; C = z; H, HT = z (if given)
  *   4 GELU_BACKWARD  d = acc * GELU'(zprev[m*ldz + n]); C = d (if C); H, HT = d (BF16, if given)
- *   with GELU the tanh form of chemgen_mlp_bias_gelu.  Asynchronous on `stream`.
+ *   with GELU the tanh form of chemgen_mlp_bias_gelu.  C (except for STORE_T) and zprev: 16-byte
+ *   aligned with ldc, ldz multiples of 4; H: 16-byte aligned with ldh a multiple of 8.
+ *   Asynchronous on `stream`.
  * chemgen_mlp_tc_error: 1 if a bounded wait inside chemgen_mlp_gemm_tc gave
  *   up (outputs incomplete), else 0, -1 on a CUDA error; reset != 0 clears it.
- * chemgen_mlp_transpose_bf16: dst[c*ldd + r] = src[r*lds + c], r < rows, c < cols. */
+ * chemgen_mlp_transpose_bf16: dst[c*ldd + r] = src[r*lds + c], r < rows, c < cols.
+ * chemgen_mlp_adam_multi: one Adam step (as chemgen_mlp_adam) over `count` <= 8 FP32 tensors
+ *   [rows[k] x cols[k]] in one launch, with weight decay decay[k] (decay may be NULL: none); the
+ *   host arrays hold device pointers.  Per tensor it also writes, where the pointer is not NULL,
+ *   wb[k] = BF16(w), wt[k][c*rows + r] = BF16(w[r][c]) and wd[k][r*2cols + c] =
+ *   wd[k][r*2cols + cols + c] = BF16(w[r][c]) (wb, wt, wd themselves may be NULL). */
 int chemgen_mlp_gemm_tc(const void* A, int64_t lda, const void* B, int64_t ldb, int M, int N, int K, int epilogue,
                         const float* bias, const float* zprev, int64_t ldz, float* C, int64_t ldc, void* H,
                         int64_t ldh, void* HT, int64_t ldt, int accumulate, void* stream);
 int chemgen_mlp_tc_error(int reset);
 int chemgen_mlp_transpose_bf16(const void* src, int64_t lds, int rows, int cols, void* dst, int64_t ldd,
                                void* stream);
+/* Fused training passes of the surrogate network (din -> 256 -> 256 -> 256 -> 64, GELU on the
+ * hidden layers), one CTA per 128 batch rows, B a multiple of 128, all BF16 operands 16-byte
+ * aligned.  chemgen_mlp_forward_tc: X [B x K0] (row stride ldx, a multiple of 8; K0 = 64, or
+ *   128 for hi + lo parts with W[0] = the first layer's weights twice side by side), W[0..3]
+ *   [N x K] BF16, b[0..3] FP32 -> ZT[l] = (H_{l-1} W_l^T + b_l)^T [256 x B] FP32, HT[l] =
+ *   GELU(Z_l)^T [256 x B] BF16 (l < 3), out = H_2 W_3^T + b_3 [B x 64] FP32 (16-byte aligned).
+ * chemgen_mlp_backward_tc: dout [B x 64] BF16, WT[1..3] = W_l^T [in x out] BF16 (WT[0] unused),
+ *   ZT[0..2] from the forward -> dZT[l] = dZ_l^T [256 x B] BF16 with dZ_2 = (dout W_3) *
+ *   GELU'(Z_2), dZ_1 = (dZ_2 W_2) * GELU'(Z_1), dZ_0 = (dZ_1 W_1) * GELU'(Z_0); gb[l][n] =
+ *   sum_m dZ_l[m][n] (FP32, 256 each, overwritten); doutT = dout^T [64 x B] BF16.
+ * Both asynchronous on `stream`; a time-out of a bounded wait sets chemgen_mlp_tc_error. */
+int chemgen_mlp_forward_tc(const void* X, int64_t ldx, int K0, const void* const* W, const float* const* b, int B,
+                           float* const* ZT, void* const* HT, float* out, void* stream);
+int chemgen_mlp_backward_tc(const void* dout, const void* const* WT, const float* const* ZT, int B,
+                            void* const* dZT, float* const* gb, void* doutT, void* stream);
+int chemgen_mlp_adam_multi(int count, float* const* w, const float* const* g, float* const* m, float* const* v,
+                           void* const* wb, void* const* wt, void* const* wd, const int* rows, const int* cols,
+                           const float* decay, const float* hyper, float b1, float b2, float eps, void* stream);
 
 int chemgen_surrogate_image_elems(void);
 int chemgen_surrogate_pack(const void* W1, const void* W2, const void* W3, const void* W4, void* img, void* stream);

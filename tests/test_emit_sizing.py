@@ -48,6 +48,28 @@ def test_emitted_launch_shape_matches_the_choice():
     assert mixed.count("__syncthreads();") >= mech.nr // E.SYNC_EVERY_MIXED
 
 
+def test_fp64_values_of_three_reactions_share_one_wait():
+    """FP64 kernel, tensor-memory mode: the values of EGP_GROUP consecutive
+    reactions (in emission order) are issued together and completed by one
+    wait whose operands are exactly those registers, and each reversible
+    reaction reads only values of its own group."""
+    mech = synthetic.gri_shape()
+    order = E.reaction_order(mech)
+    fp64 = E.emit(mech, precision="fp64")
+    G = E.EGP_GROUP
+    groups = [order[p:p + G] for p in range(0, len(order), G)]
+    with_rev = [g for g in groups if any(mech.reactions[j].reversible for j in g)]
+    waits = re.findall(r'asm volatile\("tcgen05\.wait::ld\.sync\.aligned;" : ([^:]*) :: "memory"\);', fp64)
+    assert len(waits) == len(with_rev)
+    for w, g in zip(waits, with_rev):
+        sps = {sp for j in g if mech.reactions[j].reversible
+               for sp in list(mech.reactions[j].reactants) + list(mech.reactions[j].products)}
+        assert w.count('"+r"') == 2 * len(sps)
+    assert "cgg::tm_ld(" not in fp64                # no per-reaction loads left
+    # the per-reaction form is still available
+    assert "cgg::tm_ld(" in E.emit(mech, precision="fp64", egp_group=1)
+
+
 def test_tmem_option_for_the_mixed_kernel():
     mech = synthetic.synthetic_mechanism(20, 60, 4, 4, seed=91, name="synthetic_20_60_s91")
     src = E.emit(mech, tmem=True)

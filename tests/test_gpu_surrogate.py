@@ -138,6 +138,36 @@ def test_tensor_core_training_step_matches_warp_level_path():
         assert (a - b).norm() / b.norm() < 5e-3, ((a - b).norm() / b.norm()).item()
 
 
+@pytest.mark.gpu
+def test_multi_tensor_adam_writes_the_product_operands():
+    """The one-launch Adam of the tensor-core path gives the same FP32
+    weights and moments as the per-tensor Adam, and writes the BF16 copy,
+    the transposed weights and the first layer's doubled copy that the
+    per-tensor path rebuilds with transposes."""
+    import torch
+    from chemgen_b200 import surrogate as S
+    g = torch.Generator(device="cuda").manual_seed(11)
+    nets = {tc: S.MLP(seed=2, tc=tc) for tc in (True, False)}
+    grads = [torch.randn(p.shape, device="cuda", generator=g) * 1e-2 for p in nets[True].params]
+    hyper = torch.tensor([1e-3, 1.0 / (1 - 0.9), 1.0 / (1 - 0.999)], device="cuda")
+    for tc, net in nets.items():
+        for _ in range(3):
+            net.adam(grads, hyper, wd=1e-4)
+    nets[False].refresh_operands()
+    torch.cuda.synchronize()
+    a, b = nets[True], nets[False]
+    # the two kernels may contract the update's products into FMAs differently
+    for j, (x, y) in enumerate(zip(a.params + a.m + a.v, b.params + b.m + b.v)):
+        rel = ((x - y).abs().max() / y.abs().max().clamp_min(1e-30)).item()
+        print(j, tuple(x.shape), rel)
+        assert rel < 1e-5, (j, rel)
+    for l in range(4):
+        assert torch.equal(a.Wb[l], a.W[l].to(torch.bfloat16))
+        assert torch.equal(a.WT[l], a.Wb[l].t())
+    din = S.DIN
+    assert torch.equal(a.Wd0[:, :din], a.Wb[0]) and torch.equal(a.Wd0[:, din:], a.Wb[0])
+
+
 # The kernels' GELU uses the hardware tanh approximation (relative error
 # about 2^-11); the oracle uses exact tanh.  With the BF16 roundings
 # restated, what is left is that approximation moving a fraction of the
@@ -254,6 +284,50 @@ def test_surrogate_trains_and_gains_over_exact_kernel():
     assert np.quantile(e_after, 0.9) <= np.quantile(err, 0.9)
 
 
+def test_gated_surrogate_beats_the_mixed_kernel():
+    """With the bench's training (10^7 samples, 16 epochs) and its 5 %
+    tolerance, the gated surrogate (fused inference, exact mixed kernel for
+    the points the gate sends back) is faster than the mixed kernel on all
+    points, and the error left after the gate is bounded at the 99.9th
+    percentile; the strict gate (margin 0.5) trades fallback for accuracy."""
+    import torch
+    from chemgen_b200 import surrogate as S
+    gm = GpuMechanism(synthetic.gri_shape(), generated=True)
+    sur = S.Surrogate(gm, seed=0)
+    info = sur.fit(S.TrainConfig())
+    n = 1 << 22
+    P, T, Y = sur.sample_states(n, torch.Generator(device="cuda").manual_seed(4242))
+    W64 = gm.getrates(P, T, Y, mode="fp64")
+    W = torch.empty_like(W64)
+    run = S.SurrogateGetrates(sur, tol=0.05)
+
+    def ms(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    t_mixed, t_gate = [], []
+    for _ in range(3):        # interleaved, best of three each
+        t_mixed.append(ms(lambda: gm.getrates(P, T, Y, out=W, mode="mixed")))
+        t_gate.append(ms(lambda: run(P, T, Y)))
+    nerr = lambda X: ((X - W64).abs().max(dim=0).values / W64.abs().max(dim=0).values).cpu().numpy()
+    e = nerr(run(P, T, Y))
+    strict = S.SurrogateGetrates(sur, tol=0.05, margin=0.5)
+    e_s = nerr(strict(P, T, Y))
+    print(info, "mixed ms", t_mixed, "gated ms", t_gate, "fallback", run.last_fallback, strict.last_fallback,
+          "after gate p99.9 / max", np.quantile(e, 0.999), e.max(), "strict", np.quantile(e_s, 0.999), e_s.max())
+    assert run.last_fallback < 0.01
+    assert min(t_gate) < min(t_mixed)
+    assert np.quantile(e, 0.999) < 0.15
+    assert strict.last_fallback > run.last_fallback and np.quantile(e_s, 0.999) <= np.quantile(e, 0.999)
+
+
 @pytest.fixture(scope="module")
 def small_surrogate():
     """A briefly trained network (realistic weight and output scales)."""
@@ -298,10 +372,11 @@ def test_fused_inference_matches_layer_by_layer(small_surrogate, ng):
     # output by ~1e-3,
     # i.e. a few % of wdot at that point, neither path being the exact one;
     # how many points see a flip depends on the trained network (1 % of them
-    # above 1e-2 has been seen)
+    # above 1e-2 has been seen); the median bar needs enough points to mean
+    # anything (one point can be a flipped one)
     rel = ((W2 - W1).abs().max(dim=0).values / W1.abs().max(dim=0).values).cpu().numpy()
     assert np.isfinite(rel).all()
-    assert np.median(rel) < 1e-4 and np.quantile(rel, 0.99) < 2e-2 and rel.max() < 0.1, \
+    assert (ng < 100 or np.median(rel) < 1e-4) and np.quantile(rel, 0.99) < 2e-2 and rel.max() < 0.1, \
         (np.median(rel), np.quantile(rel, 0.99), rel.max())
     assert (e2 - e1).abs().max().item() < 0.05
 
