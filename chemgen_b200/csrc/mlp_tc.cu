@@ -85,10 +85,7 @@ __global__ void __launch_bounds__(128) mlp_gemm_tc_kernel(TcArgs g) {
     uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + kStages);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * kTM, n0 = blockIdx.y * NT;
-    // this CTA's share of K (split-K: blockIdx.z of gridDim.z, whole chunks)
-    const int nkc = g.K / kKC;
-    const int per = (nkc + gridDim.z - 1) / gridDim.z;
-    const int kc0 = blockIdx.z * per, kc1 = min(nkc, kc0 + per);
+    const int kc0 = 0, kc1 = g.K / kKC;
     if (tid == 0) {
         for (int i = 0; i < kStages; ++i) um::mbar_init(&mbar[i], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -182,8 +179,7 @@ __global__ void __launch_bounds__(128) mlp_gemm_tc_kernel(TcArgs g) {
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     float* c = g.C + (int64_t)(nb + j) * g.ldc + m;
-                    if (gridDim.z > 1) atomicAdd(c, v[j]);
-                    else *c = g.accumulate ? *c + v[j] : v[j];
+                    *c = g.accumulate ? *c + v[j] : v[j];
                 }
                 continue;
             }
@@ -236,12 +232,7 @@ __global__ void __launch_bounds__(128) mlp_gemm_tc_kernel(TcArgs g) {
                 for (int c = 4 * lane; c < NT; c += 128) {
                     const float4 x = *reinterpret_cast<const float4*>(stg + r * kLd + c);
                     float* dst = g.C + (mrow0 + r) * g.ldc + n0 + c;
-                    if (gridDim.z > 1) {
-                        atomicAdd(dst, x.x);
-                        atomicAdd(dst + 1, x.y);
-                        atomicAdd(dst + 2, x.z);
-                        atomicAdd(dst + 3, x.w);
-                    } else if (g.accumulate) {
+                    if (g.accumulate) {
                         float4 y = *reinterpret_cast<const float4*>(dst);
                         y.x += x.x; y.y += x.y; y.z += x.z; y.w += x.w;
                         *reinterpret_cast<float4*>(dst) = y;
@@ -270,18 +261,10 @@ cudaError_t launch_tc(const TcArgs& a, cudaStream_t s) {
     cudaError_t e = cudaFuncSetAttribute(mlp_gemm_tc_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    // long reductions (the weight gradients, K = batch) are split over up to
-    // eight CTAs of at least two chunks each, which add their parts atomically
-    int split = 1;
-    if (a.epi == kStore || a.epi == kStoreT) split = std::max(1, std::min(8, a.K / (2 * kKC)));
-    if (split > 1 && !a.accumulate) {
-        // the parts add into zero
-        const size_t w = (size_t)(a.epi == kStore ? a.N : a.M) * sizeof(float);
-        const size_t h = (size_t)(a.epi == kStore ? a.M : a.N);
-        e = cudaMemset2DAsync(a.C, (size_t)a.ldc * sizeof(float), 0, w, h, s);
-        if (e != cudaSuccess) return e;
-    }
-    dim3 grid((unsigned)(a.M / kTM), (unsigned)(a.N / NT), (unsigned)split);
+    // one CTA per output tile over the whole of K: every sum is formed in one
+    // order, so that training is reproducible run to run (a split of K with
+    // atomic adds was ~20 % faster on the weight gradients and was not)
+    dim3 grid((unsigned)(a.M / kTM), (unsigned)(a.N / NT), 1u);
     mlp_gemm_tc_kernel<NT><<<grid, 128, smem, s>>>(a);
     return cudaGetLastError();
 }
@@ -577,8 +560,10 @@ struct BwdArgs {
     const float* ZT[3];
     int B;
     bf16* dZT[3];
-    float* gb[3];          // accumulated (atomically) column sums
+    float* gb[3];          // column sums of dZ_l
     bf16* doutT;           // [64 x B]
+    float* part;           // [3][B / 128][256] per-tile column sums
+    unsigned* count;       // tiles done (the last one forms gb and resets it)
 };
 
 __global__ void __launch_bounds__(kFT, 1) mlp_backward_fused_kernel(BwdArgs a) {
@@ -604,6 +589,8 @@ __global__ void __launch_bounds__(kFT, 1) mlp_backward_fused_kernel(BwdArgs a) {
     // dout transposed for the last layer's weight gradient, from the tile copy
     for (int n = 32 * half; n < 32 * half + 32; ++n)
         a.doutT[(int64_t)n * a.B + m] = *reinterpret_cast<const bf16*>(sX + um::kmajor_offset(row, n, kFOut));
+    __syncthreads();   // the epilogues reuse sX for the column sums
+    float* red = reinterpret_cast<float*>(sX);   // [3 layers][4 lane quadrants][256], used from step 0's epilogue
     uint32_t parity = 0;
     bool ok = true;
     for (int s = 0; s < 3 && ok; ++s) {
@@ -616,7 +603,6 @@ __global__ void __launch_bounds__(kFT, 1) mlp_backward_fused_kernel(BwdArgs a) {
         if (s < 2) fused_load(sW, a.WT[L - 1], kFHid, kFHid, kFHid);
         const float* z = a.ZT[L - 1];
         bf16* dzt = a.dZT[L - 1];
-        float* gb = a.gb[L - 1];
 #pragma unroll 1
         for (int c = 128 * half; c < 128 * half + 128; c += 16) {
             float v[16];
@@ -639,13 +625,14 @@ __global__ void __launch_bounds__(kFT, 1) mlp_backward_fused_kernel(BwdArgs a) {
                 *reinterpret_cast<uint4*>(sA + um::kmajor_offset(row, c + 8, kFHid)) =
                     make_uint4(pk[4], pk[5], pk[6], pk[7]);
             }
-            // bias gradient: the column sums of this warp's 32 rows (FP32)
+            // bias gradient: the column sums of this warp's 32 rows (FP32),
+            // kept per lane quadrant in the input buffer, idle after step 0
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
                 float t = v[j];
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-                if (lane == 0) atomicAdd(gb + c + j, t);
+                if (lane == 0) red[((L - 1) * 4 + g4) * kFHid + c + j] = t;
             }
         }
         fused_step_end();
@@ -655,6 +642,28 @@ __global__ void __launch_bounds__(kFT, 1) mlp_backward_fused_kernel(BwdArgs a) {
     um::fence_before_sync();
     __syncthreads();
     if (warp == 0) um::tmem_dealloc(tbase, 256);
+    // bias gradients in a fixed order: this tile's column sums (quadrants in
+    // order), then the last tile to finish adds the tiles' sums in order
+    __shared__ unsigned last;
+    const int nt = gridDim.x, col = tid;
+    if (ok)
+        for (int l = 0; l < 3; ++l) {
+            const float* q = red + l * 4 * kFHid + col;
+            a.part[((int64_t)l * nt + blockIdx.x) * kFHid + col] = ((q[0] + q[kFHid]) + q[2 * kFHid]) + q[3 * kFHid];
+        }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) last = atomicAdd(a.count, 1u) == (unsigned)(nt - 1);
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        for (int l = 0; l < 3; ++l) {
+            float acc = 0.0f;
+            for (int t = 0; t < nt; ++t) acc += __ldcg(a.part + ((int64_t)l * nt + t) * kFHid + col);
+            a.gb[l][col] = acc;
+        }
+        if (tid == 0) *a.count = 0u;
+    }
 }
 
 bool fused_ready() {
@@ -697,13 +706,21 @@ extern "C" int chemgen_mlp_forward_tc(const void* X, int64_t ldx, int K0, const 
     return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA;
 }
 
+extern "C" size_t chemgen_mlp_backward_tc_work_bytes(int B) {
+    return B > 0 ? (size_t)3 * ((B + kFR - 1) / kFR) * kFHid * sizeof(float) + 16 : 0;
+}
+
 extern "C" int chemgen_mlp_backward_tc(const void* dout, const void* const* WT, const float* const* ZT, int B,
-                                       void* const* dZT, float* const* gb, void* doutT, void* stream) {
-    if (!dout || !WT || !ZT || !dZT || !gb || !doutT || B <= 0 || B % kFR) return CHEMGEN_ERR_INVALID_ARGUMENT;
+                                       void* const* dZT, float* const* gb, void* doutT, void* work, void* stream) {
+    if (!dout || !WT || !ZT || !dZT || !gb || !doutT || !work || B <= 0 || B % kFR)
+        return CHEMGEN_ERR_INVALID_ARGUMENT;
     BwdArgs a{};
     a.dout = (const bf16*)dout;
     a.B = B;
     a.doutT = (bf16*)doutT;
+    a.part = (float*)work;
+    a.count = (unsigned*)((char*)work + chemgen_mlp_backward_tc_work_bytes(B) - 16);
+    if (!al16(work)) return CHEMGEN_ERR_MISALIGNED;
     for (int l = 1; l < 4; ++l) {
         if (!WT[l]) return CHEMGEN_ERR_INVALID_ARGUMENT;
         if (!al16(WT[l])) return CHEMGEN_ERR_MISALIGNED;
@@ -718,8 +735,6 @@ extern "C" int chemgen_mlp_backward_tc(const void* dout, const void* const* WT, 
     if (!al16(dout)) return CHEMGEN_ERR_MISALIGNED;
     if (!fused_ready()) return CHEMGEN_ERR_CUDA;
     cudaStream_t s = (cudaStream_t)stream;
-    for (int l = 0; l < 3; ++l)
-        if (cudaMemsetAsync(gb[l], 0, kFHid * sizeof(float), s) != cudaSuccess) return CHEMGEN_ERR_CUDA;
     mlp_backward_fused_kernel<<<B / kFR, kFT, kFSmem, s>>>(a);
     return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA;
 }

@@ -89,7 +89,9 @@ def lib() -> ctypes.CDLL:
     L.chemgen_mlp_transpose_bf16.argtypes = [vp, i64, ci, ci, vp, i64, vp]
     L.chemgen_mlp_adam_multi.argtypes = [ci, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, f32, f32, f32, vp]
     L.chemgen_mlp_forward_tc.argtypes = [vp, i64, ci, vp, vp, ci, vp, vp, vp, vp]
-    L.chemgen_mlp_backward_tc.argtypes = [vp, vp, vp, ci, vp, vp, vp, vp]
+    L.chemgen_mlp_backward_tc.argtypes = [vp, vp, vp, ci, vp, vp, vp, vp, vp]
+    L.chemgen_mlp_backward_tc_work_bytes.argtypes = [ci]
+    L.chemgen_mlp_backward_tc_work_bytes.restype = ctypes.c_size_t
     L.chemgen_surrogate_image_elems.argtypes = []
     L.chemgen_surrogate_pack.argtypes = [vp, vp, vp, vp, vp, vp]
     L.chemgen_surrogate_infer.argtypes = [vp, vp, vp, vp, vp, ci, vp, vp, i64, vp, vp, vp, vp, vp]

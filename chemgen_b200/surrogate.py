@@ -234,10 +234,15 @@ class MLP:
             check(lib().chemgen_mlp_colsum(dout_f.data_ptr(), gb[3].data_ptr(), B, dout, _stream()), "mlp_colsum")
             _transpose(X, B, w, XT)
         P = ctypes.c_void_p
+        nwork = -(-int(lib().chemgen_mlp_backward_tc_work_bytes(B)) // 4)
+        work = self._ws.get(("bwork", B))
+        if work is None:
+            work = self._ws[("bwork", B)] = torch.zeros(nwork, dtype=torch.float32, device=self.dev)
         check(lib().chemgen_mlp_backward_tc(dout_b.data_ptr(), (P * 4)(None, *[self.WT[l].data_ptr() for l in (1, 2, 3)]),
                                             (P * 3)(*[z.data_ptr() for z in self.zs]), B,
                                             (P * 3)(*[d.data_ptr() for d in dZT]),
-                                            (P * 3)(*[g.data_ptr() for g in gb[:3]]), doutT.data_ptr(), _stream()),
+                                            (P * 3)(*[g.data_ptr() for g in gb[:3]]), doutT.data_ptr(),
+                                            work.data_ptr(), _stream()),
               "mlp_backward_tc")
         fork()
         with torch.cuda.stream(side):

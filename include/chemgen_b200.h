@@ -203,12 +203,15 @@ int chemgen_mlp_transpose_bf16(const void* src, int64_t lds, int rows, int cols,
  * chemgen_mlp_backward_tc: dout [B x 64] BF16, WT[1..3] = W_l^T [in x out] BF16 (WT[0] unused),
  *   ZT[0..2] from the forward -> dZT[l] = dZ_l^T [256 x B] BF16 with dZ_2 = (dout W_3) *
  *   GELU'(Z_2), dZ_1 = (dZ_2 W_2) * GELU'(Z_1), dZ_0 = (dZ_1 W_1) * GELU'(Z_0); gb[l][n] =
- *   sum_m dZ_l[m][n] (FP32, 256 each, overwritten); doutT = dout^T [64 x B] BF16.
+ *   sum_m dZ_l[m][n] (FP32, 256 each, overwritten, summed in a fixed order); doutT = dout^T
+ *   [64 x B] BF16.  work: chemgen_mlp_backward_tc_work_bytes(B) bytes of device memory, 16-byte
+ *   aligned, zeroed before its first use and left zeroed (one call at a time per buffer).
  * Both asynchronous on `stream`; a time-out of a bounded wait sets chemgen_mlp_tc_error. */
 int chemgen_mlp_forward_tc(const void* X, int64_t ldx, int K0, const void* const* W, const float* const* b, int B,
                            float* const* ZT, void* const* HT, float* out, void* stream);
+size_t chemgen_mlp_backward_tc_work_bytes(int B);
 int chemgen_mlp_backward_tc(const void* dout, const void* const* WT, const float* const* ZT, int B,
-                            void* const* dZT, float* const* gb, void* doutT, void* stream);
+                            void* const* dZT, float* const* gb, void* doutT, void* work, void* stream);
 int chemgen_mlp_adam_multi(int count, float* const* w, const float* const* g, float* const* m, float* const* v,
                            void* const* wb, void* const* wt, void* const* wd, const int* rows, const int* cols,
                            const float* decay, const float* hyper, float b1, float b2, float eps, void* stream);

@@ -138,7 +138,38 @@ def test_tensor_core_training_step_matches_warp_level_path():
         assert (a - b).norm() / b.norm() < 5e-3, ((a - b).norm() / b.norm()).item()
 
 
-@pytest.mark.gpu
+def test_tensor_core_training_is_reproducible():
+    """Every sum of the tensor-core training step is formed in a fixed order
+    (no split reductions with atomic adds, ordered bias-gradient sums), so two
+    runs of the same steps from the same start give bit-identical weights."""
+    import torch
+    from chemgen_b200 import surrogate as S
+    from chemgen_b200.runtime import lib
+    B = 1024
+    g = torch.Generator(device="cuda").manual_seed(21)
+    Xs = [(torch.randn(B, 2 * S.DIN, device="cuda", generator=g) * 0.5).to(torch.bfloat16) for _ in range(4)]
+    Ts = [torch.randn(B, S.DOUT, device="cuda", generator=g) for _ in range(4)]
+    colw = torch.ones(S.DOUT, device="cuda")
+    hyper = torch.tensor([1e-3, 1.0 / (1 - 0.9), 1.0 / (1 - 0.999)], device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    runs = []
+    for _ in range(2):
+        net = S.MLP(seed=8, tc=True)
+        db = torch.empty(B, S.DOUT, dtype=torch.bfloat16, device="cuda")
+        df = torch.empty(B, S.DOUT, device="cuda")
+        loss = torch.zeros(1, device="cuda")
+        for step in range(12):
+            out = net.forward(Xs[step % 4])
+            assert lib().chemgen_mlp_mse_grad(out.data_ptr(), Ts[step % 4].data_ptr(), colw.data_ptr(),
+                                              db.data_ptr(), df.data_ptr(), loss.data_ptr(), B, S.DOUT, s) == 0
+            net.adam(net.backward(db, df), hyper)
+        torch.cuda.synchronize()
+        runs.append([p.clone() for p in net.params])
+    assert lib().chemgen_mlp_tc_error(1) == 0
+    for a, b in zip(*runs):
+        assert torch.equal(a, b)
+
+
 def test_multi_tensor_adam_writes_the_product_operands():
     """The one-launch Adam of the tensor-core path gives the same FP32
     weights and moments as the per-tensor Adam, and writes the BF16 copy,
