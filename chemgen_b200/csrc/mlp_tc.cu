@@ -430,12 +430,12 @@ extern "C" int chemgen_mlp_adam_multi(int count, float* const* w, const float* c
 // FP32 accumulation in 256 tensor-memory columns) against the layer's B
 // operand, which all threads copy into shared memory (16-byte cp.async into
 // the canonical K-major layout) while the previous epilogue runs.  Warp w
-// reads lane quadrant w % 4 and column half w / 4 of the accumulator.  What
+// reads lane quadrant w % 4 and column quarter w / 4 of the accumulator.  What
 // the weight-gradient products need leaves transposed, [feature][row], where
 // a warp's lanes write consecutive addresses: Z_l (FP32), H_l and dZ_l (BF16),
 // dout.  Shared memory: 64 KB activations, 32 KB input, 128 KB weights.
 namespace {
-constexpr int kFR = 128, kFT = 256, kFHid = 256, kFOut = 64;
+constexpr int kFR = 128, kFT = 512, kFHid = 256, kFOut = 64;   // 16 warps: 4 per lane quadrant
 constexpr uint32_t kFAOff = 0, kFXOff = kFR * kFHid * 2, kFWOff = kFXOff + kFR * 128 * 2,
                    kFTail = kFWOff + kFHid * kFHid * 2;
 constexpr size_t kFSmem = (size_t)kFTail + 64;
@@ -488,7 +488,7 @@ __global__ void __launch_bounds__(kFT, 1) mlp_forward_fused_kernel(FwdArgs a) {
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kFTail);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int g4 = warp & 3, half = warp >> 2, row = 32 * g4 + lane;
+    const int g4 = warp & 3, qtr = warp >> 2, row = 32 * g4 + lane;
     const int64_t m0 = (int64_t)blockIdx.x * kFR, m = m0 + row;
     if (tid == 0) {
         um::mbar_init(bar, 1);
@@ -512,20 +512,30 @@ __global__ void __launch_bounds__(kFT, 1) mlp_forward_fused_kernel(FwdArgs a) {
         // the next layer's weights stream in while this epilogue runs
         if (l < 3) fused_load(sW, a.W[l + 1], kFHid, l == 2 ? kFOut : kFHid, kFHid);
         if (l < 3) {
-            const float* bl = a.b[l];
+            const float* __restrict__ bl = a.b[l];
+            float* __restrict__ zt = a.ZT[l];
+            bf16* __restrict__ ht = a.HT[l];
 #pragma unroll 1
-            for (int c = 128 * half; c < 128 * half + 128; c += 16) {
-                float v[16];
+            for (int c = 64 * qtr; c < 64 * qtr + 64; c += 16) {
+                float bb[16], v[16];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float4 t = __ldg(reinterpret_cast<const float4*>(bl + c) + q);
+                    bb[4 * q] = t.x;
+                    bb[4 * q + 1] = t.y;
+                    bb[4 * q + 2] = t.z;
+                    bb[4 * q + 3] = t.w;
+                }
                 um::tmem_ld16(um::tmem_lane_addr(tbase, g4, c), v);
                 uint32_t pk[8];
 #pragma unroll
                 for (int j = 0; j < 16; j += 2) {
-                    const float z0 = v[j] + __ldg(bl + c + j), z1 = v[j + 1] + __ldg(bl + c + j + 1);
-                    a.ZT[l][(int64_t)(c + j) * a.B + m] = z0;
-                    a.ZT[l][(int64_t)(c + j + 1) * a.B + m] = z1;
+                    const float z0 = v[j] + bb[j], z1 = v[j + 1] + bb[j + 1];
+                    zt[(int64_t)(c + j) * a.B + m] = z0;
+                    zt[(int64_t)(c + j + 1) * a.B + m] = z1;
                     const __nv_bfloat162 h = __floats2bfloat162_rn(gelu(z0, nullptr), gelu(z1, nullptr));
-                    a.HT[l][(int64_t)(c + j) * a.B + m] = h.x;
-                    a.HT[l][(int64_t)(c + j + 1) * a.B + m] = h.y;
+                    ht[(int64_t)(c + j) * a.B + m] = h.x;
+                    ht[(int64_t)(c + j + 1) * a.B + m] = h.y;
                     pk[j / 2] = *reinterpret_cast<const uint32_t*>(&h);
                 }
                 *reinterpret_cast<uint4*>(sA + um::kmajor_offset(row, c, kFHid)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
@@ -533,8 +543,8 @@ __global__ void __launch_bounds__(kFT, 1) mlp_forward_fused_kernel(FwdArgs a) {
                     make_uint4(pk[4], pk[5], pk[6], pk[7]);
             }
         } else {
-#pragma unroll 1
-            for (int c = 32 * half; c < 32 * half + 32; c += 16) {
+            {
+                const int c = 16 * qtr;
                 float v[16];
                 um::tmem_ld16(um::tmem_lane_addr(tbase, g4, c), v);
                 float4* o = reinterpret_cast<float4*>(a.out + m * kFOut + c);
@@ -574,7 +584,7 @@ __global__ void __launch_bounds__(kFT, 1) mlp_backward_fused_kernel(BwdArgs a) {
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kFTail);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int g4 = warp & 3, half = warp >> 2, row = 32 * g4 + lane;
+    const int g4 = warp & 3, qtr = warp >> 2, row = 32 * g4 + lane;
     const int64_t m0 = (int64_t)blockIdx.x * kFR, m = m0 + row;
     if (tid == 0) {
         um::mbar_init(bar, 1);
@@ -587,7 +597,7 @@ __global__ void __launch_bounds__(kFT, 1) mlp_backward_fused_kernel(BwdArgs a) {
     um::fence_after_sync();
     const uint32_t tbase = *tslot;
     // dout transposed for the last layer's weight gradient, from the tile copy
-    for (int n = 32 * half; n < 32 * half + 32; ++n)
+    for (int n = 16 * qtr; n < 16 * qtr + 16; ++n)
         a.doutT[(int64_t)n * a.B + m] = *reinterpret_cast<const bf16*>(sX + um::kmajor_offset(row, n, kFOut));
     __syncthreads();   // the epilogues reuse sX for the column sums
     float* red = reinterpret_cast<float*>(sX);   // [3 layers][4 lane quadrants][256], used from step 0's epilogue
@@ -601,18 +611,21 @@ __global__ void __launch_bounds__(kFT, 1) mlp_backward_fused_kernel(BwdArgs a) {
         um::fence_after_sync();
         if (!ok) break;
         if (s < 2) fused_load(sW, a.WT[L - 1], kFHid, kFHid, kFHid);
-        const float* z = a.ZT[L - 1];
-        bf16* dzt = a.dZT[L - 1];
+        const float* __restrict__ z = a.ZT[L - 1];
+        bf16* __restrict__ dzt = a.dZT[L - 1];
 #pragma unroll 1
-        for (int c = 128 * half; c < 128 * half + 128; c += 16) {
-            float v[16];
+        for (int c = 64 * qtr; c < 64 * qtr + 64; c += 16) {
+            // the 16 pre-activations first (one L2 round trip for all), then the accumulator
+            float zv[16], v[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) zv[j] = __ldcg(z + (int64_t)(c + j) * a.B + m);
             um::tmem_ld16(um::tmem_lane_addr(tbase, g4, c), v);
             uint32_t pk[8];
 #pragma unroll
             for (int j = 0; j < 16; j += 2) {
                 float d0, d1;
-                gelu(z[(int64_t)(c + j) * a.B + m], &d0);
-                gelu(z[(int64_t)(c + j + 1) * a.B + m], &d1);
+                gelu(zv[j], &d0);
+                gelu(zv[j + 1], &d1);
                 v[j] *= d0;
                 v[j + 1] *= d1;
                 const __nv_bfloat162 h = __floats2bfloat162_rn(v[j], v[j + 1]);
@@ -646,7 +659,7 @@ __global__ void __launch_bounds__(kFT, 1) mlp_backward_fused_kernel(BwdArgs a) {
     // order), then the last tile to finish adds the tiles' sums in order
     __shared__ unsigned last;
     const int nt = gridDim.x, col = tid;
-    if (ok)
+    if (ok && col < kFHid)
         for (int l = 0; l < 3; ++l) {
             const float* q = red + l * 4 * kFHid + col;
             a.part[((int64_t)l * nt + blockIdx.x) * kFHid + col] = ((q[0] + q[kFHid]) + q[2 * kFHid]) + q[3 * kFHid];
@@ -655,7 +668,7 @@ __global__ void __launch_bounds__(kFT, 1) mlp_backward_fused_kernel(BwdArgs a) {
     __syncthreads();
     if (tid == 0) last = atomicAdd(a.count, 1u) == (unsigned)(nt - 1);
     __syncthreads();
-    if (last) {
+    if (last && col < kFHid) {
         __threadfence();
         for (int l = 0; l < 3; ++l) {
             float acc = 0.0f;

@@ -464,9 +464,9 @@ class Surrogate:
     # ------------------------------------------------------------- training
     def fit(self, cfg: TrainConfig = TrainConfig(), log=None, graph: bool = True) -> Dict:
         """Train on cfg.samples exact-kernel samples.  The training step (batch
-        gather, forward, loss gradient, backward, Adam) is captured once as a
-        CUDA graph and replayed; per step only the batch indices and the
-        schedule row are copied in."""
+        gather, forward, loss gradient, backward, Adam) is captured as a CUDA
+        graph of eight consecutive steps and replayed; per replay only the
+        eight steps' batch indices and schedule rows are copied in."""
         import torch
         t0 = time.perf_counter()
         Xs, Ws = self.make_dataset(cfg.samples, cfg.seed)
@@ -488,8 +488,12 @@ class Surrogate:
         steps_per_epoch = n // B
         total = steps_per_epoch * cfg.epochs
         sched = adam_schedule(total, cfg.lr, cfg.lr_final, device=self.dev)
-        hyper = torch.empty(3, device=self.dev)
-        idx = torch.zeros(B, dtype=torch.int64, device=self.dev)
+        # one CUDA graph holds `chunk` consecutive training steps, each with its
+        # own row of batch indices and of the schedule; per replay the host
+        # copies in `chunk` rows of each, so its per-step cost stays small
+        chunk = 8 if graph else 1
+        hyper = torch.empty((chunk, 3), device=self.dev)
+        idx = torch.zeros((chunk, B), dtype=torch.int64, device=self.dev)
         xb = torch.empty((B, X.shape[1]), dtype=X.dtype, device=self.dev)
         tb = torch.empty((B, DOUT), dtype=torch.float32, device=self.dev)
         loss = torch.zeros(1, device=self.dev)
@@ -497,14 +501,14 @@ class Surrogate:
         dout_f = torch.empty((B, DOUT), dtype=torch.float32, device=self.dev)
         gen = torch.Generator(device=self.dev).manual_seed(cfg.seed + 1)
 
-        def body():
-            torch.index_select(X, 0, idx, out=xb)
-            torch.index_select(Tg, 0, idx, out=tb)
+        def body(k):
+            torch.index_select(X, 0, idx[k], out=xb)
+            torch.index_select(Tg, 0, idx[k], out=tb)
             out = self.net.forward(xb)
             check(lib().chemgen_mlp_mse_grad(out.data_ptr(), tb.data_ptr(), self.colw.data_ptr(), dout_b.data_ptr(),
                                              dout_f.data_ptr(), loss.data_ptr(), B, DOUT, _stream()), "mse_grad")
             grads = self.net.backward(dout_b, dout_f)
-            self.net.adam(grads, hyper, cfg.weight_decay)
+            self.net.adam(grads, hyper[k], cfg.weight_decay)
 
         g = None
         step = 0
@@ -512,24 +516,32 @@ class Surrogate:
         for ep in range(cfg.epochs):
             perm = torch.randperm(n, device=self.dev, generator=gen)
             loss.zero_()
-            for b in range(steps_per_epoch):
-                idx.copy_(perm[b * B:(b + 1) * B])
-                hyper.copy_(sched[step])
-                if g is not None:
+            b = 0
+            while b < steps_per_epoch:
+                if g is not None and b + chunk <= steps_per_epoch:
+                    idx.copy_(perm[b * B:(b + chunk) * B].view(chunk, B))
+                    hyper.copy_(sched[step:step + chunk])
                     g.replay()
-                else:
-                    body()
-                    if graph and step == 2:
-                        # capture after a few eager steps, once every buffer exists
-                        torch.cuda.synchronize(self.dev)
-                        side = torch.cuda.Stream(device=self.dev)
-                        side.wait_stream(torch.cuda.current_stream())
-                        g = torch.cuda.CUDAGraph()
-                        with torch.cuda.stream(side):
-                            with torch.cuda.graph(g, stream=side):
-                                body()
-                        torch.cuda.current_stream().wait_stream(side)
+                    step += chunk
+                    b += chunk
+                    continue
+                # single eager steps: the first few (every buffer comes to
+                # exist) and an epoch's last steps short of a whole replay
+                idx[0].copy_(perm[b * B:(b + 1) * B])
+                hyper[0].copy_(sched[step])
+                body(0)
                 step += 1
+                b += 1
+                if graph and g is None and step == 3:
+                    torch.cuda.synchronize(self.dev)
+                    side = torch.cuda.Stream(device=self.dev)
+                    side.wait_stream(torch.cuda.current_stream())
+                    g = torch.cuda.CUDAGraph()
+                    with torch.cuda.stream(side):
+                        with torch.cuda.graph(g, stream=side):
+                            for k in range(chunk):
+                                body(k)
+                    torch.cuda.current_stream().wait_stream(side)
             self.history.append(loss.item() / max(steps_per_epoch, 1))
             if log:
                 log(f"epoch {ep}: loss {self.history[-1]:.4e}")
