@@ -482,7 +482,7 @@ class _Emitter:
             sgn = ""
         body.append(f"double rr = {sgn}cgg::rate2(akf, {cf}, {-CSCALE_LOG2 * of});")
         if r.reversible:
-            if self.tmem:
+            if self.tmem and not self._egp_ready:
                 body += self.load_egp(r)
             body.append(f"rr -= {sgn}cgg::rate2(akf + {self.gsum(r)}, {cb}, {-CSCALE_LOG2 * ob});")
         body += self.scatter(r, "rr")
@@ -508,7 +508,7 @@ class _Emitter:
             body += self.falloff64(r)
         qf = f"kf*{self.prod(r.reactants, C)}"
         if r.reversible:
-            if self.tmem:
+            if self.tmem and not self._egp_ready:
                 body += self.load_egp(r)
             body.append(f"const double rr = {qf} - kf*({self.prod(r.reactants, E)})*rcp({self.prod(r.products, E)})"
                         f"*{self.prod(r.products, C)};")
@@ -661,7 +661,7 @@ class _Emitter:
                 if new:
                     L.append("  double " + ", ".join(f"w{k} = 0.0" for k in new) + ";")
                     declared.update(new)
-            if not mixed and self.egp_group > 1 and p % self.egp_group == 0:
+            if self.egp_group > 1 and p % self.egp_group == 0:
                 L += ["  " + x for x in self.group_egp(p, [self.mech.reactions[jj]
                                                             for jj in order[p:p + self.egp_group]])]
             if rev_pos and r.reversible:
@@ -740,7 +740,7 @@ PRECISIONS = {"fp64": (True, False), "mixed": (False, True), "both": (True, True
 def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = None,
          sync_every: Optional[int] = None, precision: str = "both", tmem: Optional[bool] = None,
          live_order: bool = True, exp_noinline: bool = False, live_order_mixed: Optional[bool] = False,
-         tm_prefetch: bool = False, egp_group: Optional[int] = None) -> str:
+         tm_prefetch: bool = False, egp_group: Optional[int] = None, egp_group_mixed: int = 1) -> str:
     """CUDA source of the mechanism's kernels: `precision` selects the FP64
     kernel, the mixed one or both; a mode without a generated kernel runs on
     the table-driven kernels."""
@@ -760,7 +760,7 @@ def emit(mech: Mechanism, name: Optional[str] = None, block: Optional[int] = Non
     em32 = _Emitter(mech, block or choose_block(mech.ns, True, tm32),
                     SYNC_EVERY_MIXED if sync_every is None else sync_every, tmem=tm32,
                     live_order=live_order if live_order_mixed is None else live_order_mixed,
-                    exp_noinline=exp_noinline)
+                    exp_noinline=exp_noinline, egp_group=egp_group_mixed)
     ident = "".join(ch if ch.isalnum() else "_" for ch in (name or mech.name))
     src = [
         f"// Generated by chemgen_b200 (generate_chemistry.py --language cuda --precision {precision}) for mechanism '{mech.name}':",
