@@ -95,15 +95,20 @@ def test_each_wdot_is_stored_once_after_its_last_reaction():
     mech = synthetic.gri_shape()
     src = E.emit(mech, precision="fp64")
     body = src.split("cg_gen_fp64(", 1)[1].split("\n}\n", 1)[0]
-    stores = re.findall(r"wdot\[\(int64_t\)(\d+) \* ng \+ i\] = (w\d+|0\.0);", body)
+    # outputs leave with streaming stores (evict-first), as the inputs arrive with streaming loads
+    stores = re.findall(r"__stcs\(wdot \+ \(int64_t\)(\d+) \* ng \+ i, (w\d+|0\.0)\);", body)
     assert sorted(int(k) for k, _ in stores) == list(range(mech.ns))
+    assert "wdot[" not in body and "Y[" not in body and body.count("__ldcs(Y + ") == mech.ns
     for k, v in stores:
         if v != "0.0":
             assert v == f"w{k}"
             decl = body.index(f" w{k} = 0.0")
             last_use = max(body.rfind(f"w{k} += "), body.rfind(f"w{k} -= "), body.rfind(f"w{k} = fma("))
-            store = body.index(f"wdot[(int64_t){k} * ng + i] = w{k};")
+            store = body.index(f"__stcs(wdot + (int64_t){k} * ng + i, w{k});")
             assert decl < last_use < store
+    # the plain form is still available
+    plain = E.emit(mech, precision="fp64", stream_io=False)
+    assert "__stcs(" not in plain and f"wdot[(int64_t)0 * ng + i] = " in plain
 
 
 @pytest.mark.slow
