@@ -37,7 +37,8 @@ SYNC_EVERY = 96           # reactions between block barriers, FP64 kernel (B200 
 # (B200 at 53/325, 2^20 points: 1 -> 509-530, 3 -> 541-554 Mpts/s with barriers every 64-96
 # reactions or none; 2, 4 and 6 gained less)
 EGP_GROUP = 3
-SYNC_EVERY_MIXED = 24     # mixed kernel (B200 sweep at 53/325: 16..96, best 24-48)
+SYNC_EVERY_MIXED = 96     # mixed kernel (B200 sweeps at 53/325, 16 warps, streaming I/O: 12..96 and
+                          # none within 3 %; 24 was best at 11 warps before the streaming hints)
 SMEM_BUDGET = 220 * 1024  # dynamic shared memory per block
 REG_FILE = 65536          # 32-bit registers per SM
 MAX_BLOCK = 512           # 16 warps; beyond this the 53-species kernels spill heavily
@@ -734,13 +735,14 @@ def choose_block(ns: int, mixed: bool, tmem: bool = False) -> int:
 
 
 def use_tmem(ns: int, mixed: bool = False) -> bool:
-    """FP64 kernel: EGp moves to tensor memory when that lets the block grow
-    and the columns fit.  The mixed kernel keeps its Gibbs terms in shared
-    memory by default: at 53/325 the tensor-memory form (16 warps, 761-770
-    Mpts/s on B200) lost to 11 warps in shared memory (795 Mpts/s), its extra
-    load instructions outweighing the extra warps; emit(tmem=True) still
-    selects it."""
-    if ns > MAX_REG_SPECIES or mixed:
+    """The per-point Gibbs array (EGp for the FP64 kernel, the log2 Gibbs
+    terms for the mixed one) moves to tensor memory when that lets the block
+    grow and the columns fit.  Measured on B200 at 53/325, 2^20 points, with
+    the streaming input/output hints: mixed 16 warps (tensor memory) 1055
+    against 11 warps (shared memory) 830 Mpts/s.  Before those hints the
+    kernels were bound by instruction fetches from DRAM and the shared-memory
+    form had won (795 against 761-770)."""
+    if ns > MAX_REG_SPECIES:
         return False
     b = choose_block(ns, mixed, True)
     return b > choose_block(ns, mixed) and -(-b // 128) * 2 * ns <= 512

@@ -24,9 +24,11 @@ def test_block_fits_every_resource(ns, mixed):
 
 
 def test_53_species_choices():
-    # FP64: EGp in tensor memory, 16 warps; mixed: both arrays in shared memory, 11 warps
+    # both kernels: the Gibbs array in tensor memory, 16 warps (the mixed kernel's shared-memory
+    # form, both arrays there, would hold 11)
     assert E.use_tmem(53, False) and E.choose_block(53, False, True) == 512
-    assert not E.use_tmem(53, True) and E.choose_block(53, True) == 352
+    assert E.use_tmem(53, True) and E.choose_block(53, True, True) == 512
+    assert E.choose_block(53, True) == 352
     # small mechanisms need no tensor memory to reach the block cap
     assert not E.use_tmem(10, False) and E.choose_block(10, False) == 512
 
@@ -35,9 +37,9 @@ def test_emitted_launch_shape_matches_the_choice():
     mech = synthetic.gri_shape()
     src = E.emit(mech)
     shapes = dict(re.findall(r"__launch_bounds__\((\d+), 1\) (cg_gen_\w+)\(", src)[i][::-1] for i in range(2))
-    assert shapes == {"cg_gen_fp64": "512", "cg_gen_mixed": "352"}
-    # one tensor-memory allocation (FP64 kernel), freed at its end; columns 2 ns per warp slot
-    assert src.count("cgg::tm_alloc(&tm_slot, 512u)") == 1 and src.count("cgg::tm_free(tbase, 512u)") == 1
+    assert shapes == {"cg_gen_fp64": "512", "cg_gen_mixed": "512"}
+    # one tensor-memory allocation per kernel, freed at its end; columns 2 ns per warp slot
+    assert src.count("cgg::tm_alloc(&tm_slot, 512u)") == 2 and src.count("cgg::tm_free(tbase, 512u)") == 2
     assert "cgg::tm_thread_base(tbase, 106)" in src
     # every EGp load of a reaction stays inside the warp slot's columns
     offs = [int(x) for x in re.findall(r"tw \+ (\d+)u", src)]
