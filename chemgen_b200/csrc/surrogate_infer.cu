@@ -62,14 +62,21 @@ __device__ __forceinline__ uint32_t pack2(bf16 lo, bf16 hi) {
     return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
 }
 
-// The network's activation exactly as in training (chemgen_mlp_bias_gelu):
-// GELU in tanh form with the hardware tanh approximation, one MUFU operation.
-__device__ __forceinline__ float gelu_fast(float z) {
-    const float u = 0.7978845608028654f * fmaf(0.044715f * z * z, z, z);
-    float t;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
-    const float hz = 0.5f * z;
-    return fmaf(hz, t, hz);
+// The network's activation exactly as in training (mlp_act.cuh: GELU in tanh
+// form, 0.5 z (1 + tanh(k0 (z + k1 z^3))), the hardware tanh approximation),
+// on two values with the packed FP32 instructions of sm_100 (mul/fma .f32x2):
+// the same operations in the same order, so the same roundings, in half the
+// issue slots; the tanh stays one MUFU operation per value.
+__device__ __forceinline__ float2 gelu_fast2(float2 z) {
+    const float2 k1 = make_float2(0.044715f, 0.044715f), k0 = make_float2(0.7978845608028654f, 0.7978845608028654f);
+    const float2 half = make_float2(0.5f, 0.5f);
+    const float2 z3 = __fmul2_rn(__fmul2_rn(k1, z), z);           // 0.044715 z z
+    const float2 u = __fmul2_rn(k0, __ffma2_rn(z3, z, z));        // k0 fma(.., z, z)
+    float2 t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t.x) : "f"(u.x));
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t.y) : "f"(u.y));
+    const float2 hz = __fmul2_rn(half, z);
+    return __ffma2_rn(hz, t, hz);
 }
 
 // 16 accumulators + bias -> GELU -> BF16, two 16-byte stores (8 columns each).
@@ -79,10 +86,14 @@ __device__ __forceinline__ void gelu_store16(const uint32_t* r, const float* __r
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const float4 bb = __ldg(reinterpret_cast<const float4*>(b) + q);
-        const float z0 = __uint_as_float(r[4 * q]) + bb.x, z1 = __uint_as_float(r[4 * q + 1]) + bb.y;
-        const float z2 = __uint_as_float(r[4 * q + 2]) + bb.z, z3 = __uint_as_float(r[4 * q + 3]) + bb.w;
-        pk[2 * q] = pack2(__float2bfloat16(gelu_fast(z0)), __float2bfloat16(gelu_fast(z1)));
-        pk[2 * q + 1] = pack2(__float2bfloat16(gelu_fast(z2)), __float2bfloat16(gelu_fast(z3)));
+        const float2 z01 = __fadd2_rn(make_float2(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1])),
+                                      make_float2(bb.x, bb.y));
+        const float2 z23 = __fadd2_rn(make_float2(__uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3])),
+                                      make_float2(bb.z, bb.w));
+        const float2 h01 = gelu_fast2(z01), h23 = gelu_fast2(z23);
+        const __nv_bfloat162 p01 = __floats2bfloat162_rn(h01.x, h01.y), p23 = __floats2bfloat162_rn(h23.x, h23.y);
+        pk[2 * q] = *reinterpret_cast<const uint32_t*>(&p01);
+        pk[2 * q + 1] = *reinterpret_cast<const uint32_t*>(&p23);
     }
     *reinterpret_cast<uint4*>(dst0) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
     *reinterpret_cast<uint4*>(dst1) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
