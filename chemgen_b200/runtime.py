@@ -96,6 +96,11 @@ def lib() -> ctypes.CDLL:
     L.chemgen_surrogate_pack.argtypes = [vp, vp, vp, vp, vp, vp]
     L.chemgen_surrogate_infer.argtypes = [vp, vp, vp, vp, vp, ci, vp, vp, i64, vp, vp, vp, vp, vp]
     L.chemgen_surrogate_infer_error.argtypes = [ci]
+    L.chemgen_gate_select.argtypes = [vp, f32, i64, vp, i64, vp, vp]
+    L.chemgen_gate_gather.argtypes = [vp, vp, vp, ci, i64, vp, vp, i64, vp, vp, vp, vp]
+    L.chemgen_gate_scatter.argtypes = [vp, ci, i64, vp, vp, vp, i64, vp]
+    for f in ("chemgen_gate_select", "chemgen_gate_gather", "chemgen_gate_scatter"):
+        getattr(L, f).restype = ci
     for f in ("chemgen_mlp_gemm", "chemgen_mlp_gemm_tc", "chemgen_mlp_tc_error", "chemgen_mlp_transpose_bf16",
               "chemgen_mlp_adam_multi", "chemgen_mlp_forward_tc", "chemgen_mlp_backward_tc",
               "chemgen_mlp_bias_gelu", "chemgen_mlp_gelu_backward", "chemgen_mlp_mse_grad",

@@ -730,24 +730,93 @@ class SurrogateGetrates:
     under-estimates some states at the edges of the training distribution;
     a margin of 0.5 (a factor 3.2 on the estimate) trades more fallback for
     a bounded worst case (on B200 at 53/325 with the default training:
-    fallback 0.15 % -> 6-29 %, max normwise error after fallback 15 -> ~1)."""
+    fallback 0.15 % -> 6-29 %, max normwise error after fallback 15 -> ~1).
 
-    def __init__(self, sur: Surrogate, tol: float, exact_mode: str = "mixed", margin: float = 0.0):
+    On CUDA tensors the gate runs on the device behind the fused inference
+    kernel, with no host round trip in between: chemgen_gate_select lists the
+    failing points, chemgen_gate_gather packs their states into a batch of
+    `cap` points, the exact kernel runs on that batch and chemgen_gate_scatter
+    writes its results over the surrogate's.  The host reads the count once,
+    at the end of the call; if more points failed than the batch holds, all
+    failing points go through the host path (`_host_gate`) and the batch
+    grows for the next call.  The batch starts at one wave of the exact
+    kernel (65536 points) because an exact launch over fewer points takes
+    about as long: a point's latency, not the batch size, sets its time."""
+
+    MIN_CAP = 1 << 16
+
+    def __init__(self, sur: Surrogate, tol: float, exact_mode: str = "mixed", margin: float = 0.0,
+                 cap: int = 0):
         self.sur = sur
         self.tol = tol
         self.exact_mode = exact_mode
         self.margin = margin
         self.last_fallback = 0.0
+        self._cap = cap
+        self._bufs = None
 
-    def __call__(self, P, T, Y):
+    @property
+    def threshold(self) -> float:
+        return math.log10(self.tol) - self.margin
+
+    def _host_gate(self, P, T, Y, W, est):
+        """Host-side gate: every failing point through the exact kernel."""
         import torch
-        # the fused kernel folds the training-support check into the estimate
-        W, est = self.sur.predict(P, T, Y, check_range=True)
-        ok = est <= math.log10(self.tol) - self.margin
+        ok = est <= self.threshold
         bad = torch.nonzero(~ok).flatten()
         if bad.numel():
             Pb, Tb = P.index_select(0, bad).contiguous(), T.index_select(0, bad).contiguous()
             Yb = Y.index_select(1, bad).contiguous()
             W[:, bad] = self.sur.gm.getrates(Pb, Tb, Yb, mode=self.exact_mode)
-        self.last_fallback = bad.numel() / max(T.numel(), 1)
+        return bad.numel()
+
+    def _buffers(self, ng: int):
+        """Batch buffers of the device gate; the unused slots always hold a
+        valid state (1 atm, 1000 K, equal mass fractions, or a state of an
+        earlier call), so the exact kernel's work on them is harmless."""
+        import torch
+        cap = min(ng, max(self._cap, self.MIN_CAP))
+        b = self._bufs
+        if b is None or b["cap"] != cap:
+            dev, ns = self.sur.dev, self.sur.ns
+            f64 = dict(dtype=torch.float64, device=dev)
+            b = {"cap": cap,
+                 "P": torch.full((cap,), 1013250.0, **f64), "T": torch.full((cap,), 1000.0, **f64),
+                 "Y": torch.full((ns, cap), 1.0 / ns, **f64), "W": torch.empty((ns, cap), **f64),
+                 "idx": torch.empty(cap, dtype=torch.int64, device=dev),
+                 "count": torch.zeros(1, dtype=torch.int64, device=dev),
+                 "count_host": torch.zeros(1, dtype=torch.int64, pin_memory=True),
+                 "done": torch.cuda.Event()}
+            self._bufs = b
+        return b
+
+    def __call__(self, P, T, Y):
+        import torch
+        P, T, Y = P.contiguous(), T.contiguous(), Y.contiguous()
+        # the fused kernel folds the training-support check into the estimate
+        W, est = self.sur.predict(P, T, Y, check_range=True)
+        ng = T.numel()
+        if not (W.is_cuda and ng):
+            self.last_fallback = self._host_gate(P, T, Y, W, est) / max(ng, 1)
+            return W
+        b = self._buffers(ng)
+        cap, ns, s = b["cap"], self.sur.ns, _stream()
+        check(lib().chemgen_gate_select(est.data_ptr(), self.threshold, ng, b["idx"].data_ptr(), cap,
+                                        b["count"].data_ptr(), s), "gate_select")
+        check(lib().chemgen_gate_gather(P.data_ptr(), T.data_ptr(), Y.data_ptr(), ns, ng, b["idx"].data_ptr(),
+                                        b["count"].data_ptr(), cap, b["P"].data_ptr(), b["T"].data_ptr(),
+                                        b["Y"].data_ptr(), s), "gate_gather")
+        self.sur.gm.getrates(b["P"], b["T"], b["Y"], out=b["W"], mode=self.exact_mode)
+        check(lib().chemgen_gate_scatter(b["W"].data_ptr(), ns, cap, b["idx"].data_ptr(), b["count"].data_ptr(),
+                                         W.data_ptr(), ng, s), "gate_scatter")
+        b["count_host"].copy_(b["count"], non_blocking=True)
+        b["done"].record()
+        b["done"].synchronize()
+        n = int(b["count_host"][0])
+        if n > cap:
+            # more failing points than the batch holds: all of them through
+            # the host path, and a larger batch next time
+            self._host_gate(P, T, Y, W, est)
+            self._cap = min(ng, -(-(n + n // 4) // self.MIN_CAP) * self.MIN_CAP)
+        self.last_fallback = n / ng
         return W

@@ -223,6 +223,26 @@ int chemgen_surrogate_infer(const void* img, const float* bias, const float* nor
                             const double* Y, double* wdot, float* err_est, const double* range, void* stream);
 int chemgen_surrogate_infer_error(int reset);
 
+/* Per-point error gate of the surrogate on the device (no counterpart in the
+ * reference): the points whose error estimate fails are gathered into a
+ * compact batch for the exact kernel and its results scattered back, all
+ * asynchronous on `stream`, so the host need not read the count between the
+ * surrogate's kernel and the exact one.
+ * chemgen_gate_select: *count = the number of points i < ng with !(est[i] <= thr) (NaN fails);
+ *   the first min(*count, cap) of them get their index in idx[0, cap), in no fixed order.
+ *   A count above cap leaves the rest unlisted: the caller reads *count afterwards and treats
+ *   them itself.  *count is zeroed by the call.
+ * chemgen_gate_gather: for j < min(*count, cap): Pc[j] = P[idx[j]], Tc[j] = T[idx[j]],
+ *   Yc[k*cap + j] = Y[k*ng + idx[j]]; slots past the count are left as they are.
+ * chemgen_gate_scatter: for j < min(*count, cap): W[k*ng + idx[j]] = Wc[k*cap + j].
+ * Pointers are device pointers, 8-byte aligned. */
+int chemgen_gate_select(const float* est, float thr, int64_t ng, int64_t* idx, int64_t cap, uint64_t* count,
+                        void* stream);
+int chemgen_gate_gather(const double* P, const double* T, const double* Y, int ns, int64_t ng, const int64_t* idx,
+                        const uint64_t* count, int64_t cap, double* Pc, double* Tc, double* Yc, void* stream);
+int chemgen_gate_scatter(const double* Wc, int ns, int64_t cap, const int64_t* idx, const uint64_t* count,
+                         double* W, int64_t ng, void* stream);
+
 /* FP64 getrates that allocates no device memory (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc while they run -- a
  * solver that owns the device memory pool or forbids allocation (and the

@@ -479,3 +479,82 @@ def test_checkpoint_round_trip(tmp_path):
     other = GpuMechanism(synthetic.h2o2_10sp())
     with pytest.raises(ValueError):
         S.Surrogate(other).load(str(tmp_path / "sur.pt"))
+
+
+@pytest.mark.parametrize("ng,cap", [(1, 1), (1000, 1000), (100_003, 4096), (100_003, 65536)])
+def test_gate_kernels_select_gather_scatter(ng, cap):
+    """chemgen_gate_select lists exactly the points whose estimate is not
+    below the threshold (NaN included) and counts them all, also past the
+    batch; gather and scatter move exactly the listed points' states and
+    results."""
+    import torch
+    from chemgen_b200.runtime import lib
+    dev = "cuda"
+    g = torch.Generator(device=dev).manual_seed(ng + cap)
+    ns = 7
+    est = torch.randn(ng, generator=g, device=dev, dtype=torch.float32) - 2.0
+    est[::97] = float("nan")
+    thr = -1.5
+    P = torch.rand(ng, generator=g, device=dev, dtype=torch.float64)
+    T = torch.rand(ng, generator=g, device=dev, dtype=torch.float64)
+    Y = torch.rand((ns, ng), generator=g, device=dev, dtype=torch.float64)
+    idx = torch.full((cap,), -1, dtype=torch.int64, device=dev)
+    count = torch.full((1,), 12345, dtype=torch.int64, device=dev)
+    s = torch.cuda.current_stream().cuda_stream
+    assert lib().chemgen_gate_select(est.data_ptr(), thr, ng, idx.data_ptr(), cap, count.data_ptr(), s) == 0
+    want = torch.nonzero(~(est <= thr)).flatten()
+    n = int(count.item())
+    assert n == want.numel()
+    m = min(n, cap)
+    got = idx[:m].sort().values
+    assert torch.equal(torch.unique(got), got)            # no point twice
+    assert torch.isin(got, want).all() and (idx[m:] == -1).all()
+    if n <= cap:
+        assert torch.equal(got, want)
+    Pc = torch.full((cap,), -7.0, dtype=torch.float64, device=dev)
+    Tc, Yc = Pc.clone(), torch.full((ns, cap), -7.0, dtype=torch.float64, device=dev)
+    assert lib().chemgen_gate_gather(P.data_ptr(), T.data_ptr(), Y.data_ptr(), ns, ng, idx.data_ptr(),
+                                     count.data_ptr(), cap, Pc.data_ptr(), Tc.data_ptr(), Yc.data_ptr(), s) == 0
+    sel = idx[:m]
+    assert torch.equal(Pc[:m], P[sel]) and torch.equal(Tc[:m], T[sel]) and torch.equal(Yc[:, :m], Y[:, sel])
+    assert (Pc[m:] == -7.0).all() and (Yc[:, m:] == -7.0).all()     # slots past the count untouched
+    Wc = torch.rand((ns, cap), generator=g, device=dev, dtype=torch.float64)
+    W = torch.zeros((ns, ng), dtype=torch.float64, device=dev)
+    assert lib().chemgen_gate_scatter(Wc.data_ptr(), ns, cap, idx.data_ptr(), count.data_ptr(), W.data_ptr(),
+                                      ng, s) == 0
+    ref = torch.zeros_like(W)
+    ref[:, sel] = Wc[:, :m]
+    assert torch.equal(W, ref)
+    # arguments
+    assert lib().chemgen_gate_select(0, thr, ng, idx.data_ptr(), cap, count.data_ptr(), s) == 1
+    assert lib().chemgen_gate_scatter(Wc.data_ptr(), 0, cap, idx.data_ptr(), count.data_ptr(), W.data_ptr(),
+                                      ng, s) == 1
+
+
+def test_device_gate_matches_host_gate(small_surrogate):
+    """The device-side gate (no host round trip between the fused kernel and
+    the exact one) gives bit for bit what the host-side gate gives, with the
+    batch large enough, with more failing points than the batch holds (the
+    call then finishes on the host path and grows the batch) and again after
+    that growth; the fallback rate is the count of failing points."""
+    import torch
+    from chemgen_b200 import surrogate as S
+    sur = small_surrogate
+    ng = (1 << 18) + 77
+    P, T, Y = sur.sample_states(ng, torch.Generator(device="cuda").manual_seed(31))
+    W0, est = sur.predict(P, T, Y, check_range=True)
+    for q in (0.02, 0.6):               # 2 % and 60 % of the points fail
+        tol = 10 ** float(torch.quantile(est.double(), 1.0 - q))
+        host = S.SurrogateGetrates(sur, tol=tol)
+        Wh, eh = sur.predict(P, T, Y, check_range=True)
+        nh = host._host_gate(P, T, Y, Wh, eh)
+        dev = S.SurrogateGetrates(sur, tol=tol)
+        for call in range(2):
+            Wd = dev(P, T, Y)
+            torch.cuda.synchronize()
+            assert torch.equal(Wd, Wh), (q, call)
+            assert dev.last_fallback == pytest.approx(nh / ng)
+        if q > 0.5:
+            assert dev._bufs["cap"] >= nh          # grown after the first call's overflow
+        else:
+            assert dev._bufs["cap"] == dev.MIN_CAP
