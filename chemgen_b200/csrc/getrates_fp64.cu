@@ -405,6 +405,30 @@ __device__ __forceinline__ StFast load_stfast(const StFast* p) {
     return f;
 }
 
+// M = ctot + sum_e (eff_e - 1) C[sp_e] of reaction r (third_body.j2:18-31), the
+// efficiencies taken four at a time so that their loads are in flight
+// together; the sum keeps the table's order.
+__device__ __forceinline__ double staged_m(const DevMech& m, int r, double ctot, const double* C) {
+    double M = ctot;
+    const int e1 = __ldg(m.eff_ptr + r + 1);
+    for (int e = __ldg(m.eff_ptr + r); e < e1; e += 4) {
+        int sp[4];
+        double ev[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const bool ok = e + u < e1;
+            sp[u] = ok ? __ldg(m.eff_sp + e + u) : 0;
+            ev[u] = ok ? __ldg(m.eff_val + e + u) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const double cv = C[sp[u] * kStTile];
+            if (e + u < e1) M = fma(ev[u], cv, M);
+        }
+    }
+    return M;
+}
+
 template <int W, int KPW>
 __global__ void __launch_bounds__(32 * W, 1)
     getrates_fp64_staged(DevMech m, int R, int nchunk, const int* __restrict__ cptr, const int* __restrict__ cer,
@@ -473,6 +497,9 @@ __global__ void __launch_bounds__(32 * W, 1)
                 const int r = c * R + rl;
                 double q = 0.0;
                 const StFast F = load_stfast(fast + (r < m.nr ? r : 0));
+                // the warp's next record moves into L1 while this one is evaluated
+                // (a prefetch: no registers held)
+                if (r + W < m.nr) asm volatile("prefetch.global.L1 [%0];" ::"l"(fast + r + W));
                 if (r < m.nr && (F.flags & kStOn)) {
                     const double kf = cgm::cg_exp_clamped(fma(F.b, pt.lnT, F.lnA) - F.theta * pt.invT);
                     q = kf * C[F.sr[0] * kStTile] * C[F.sr[1] * kStTile] * C[F.sr[2] * kStTile];
@@ -482,12 +509,7 @@ __global__ void __launch_bounds__(32 * W, 1)
                         q -= kf * num * rcp_nr(den) * C[F.sp[0] * kStTile] * C[F.sp[1] * kStTile] *
                              C[F.sp[2] * kStTile];
                     }
-                    if (F.flags & kStThird) {
-                        double M = ctot;
-                        for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
-                            M = fma(__ldg(m.eff_val + e), C[__ldg(m.eff_sp + e) * kStTile], M);
-                        q *= M;
-                    }
+                    if (F.flags & kStThird) q *= staged_m(m, r, ctot, C);
                     if (F.flags & kStNeg) q = -q;
                 } else if (r < m.nr) {
                     const DRxn Rx = load_rxn(m.rxn + r);
@@ -496,18 +518,14 @@ __global__ void __launch_bounds__(32 * W, 1)
                     if (kind == CG_STANDARD) {
                         q = net_rate<kStTile>(m, Rx, arrhenius(Rx.lnA, Rx.b, Rx.theta, Rx.sgn, pt), 1.0, C, E);
                     } else if (kind == CG_THIRD_BODY) {
-                        double M = ctot;
-                        for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
-                            M = fma(__ldg(m.eff_val + e), C[__ldg(m.eff_sp + e) * kStTile], M);
+                        const double M = staged_m(m, r, ctot, C);
                         q = net_rate<kStTile>(m, Rx, arrhenius(Rx.lnA, Rx.b, Rx.theta, Rx.sgn, pt), M, C, E);
                     } else if (kind == CG_PLOG) {
                         q = net_rate<kStTile>(m, Rx, plog_kf(m, Rx.aux, Pp, lnP, pt), 1.0, C, E);
                     } else {
                         const DFall f = load_fall(m.fall + Rx.aux);
                         const double x2 = __ldg(&m.fall2[Rx.aux].T2);
-                        double M = ctot;
-                        for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
-                            M = fma(__ldg(m.eff_val + e), C[__ldg(m.eff_sp + e) * kStTile], M);
+                        const double M = staged_m(m, r, ctot, C);
                         q = net_rate<kStTile>(m, Rx, falloff_kf(kind, Rx.flags, Rx, f, x2, M, pt), 1.0, C, E);
                     }
                 }
@@ -520,9 +538,24 @@ __global__ void __launch_bounds__(32 * W, 1)
             for (int j = 0; j < KPW; ++j) {
                 const int k = warp + j * W;
                 if (k < ns) {
+                    // entries four at a time, their loads in flight together;
+                    // the sum keeps the list's order
                     const int e1 = __ldg(cp + k + 1);
-                    for (int e = __ldg(cp + k); e < e1; ++e)
-                        acc[j] = fma(__ldg(cnu + e), sQ[__ldg(cer + e) * kStTile + lane], acc[j]);
+                    for (int e = __ldg(cp + k); e < e1; e += 4) {
+                        int ix[4];
+                        double nu[4];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const bool ok = e + u < e1;
+                            ix[u] = ok ? __ldg(cer + e + u) : 0;
+                            nu[u] = ok ? __ldg(cnu + e + u) : 0.0;
+                        }
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const double qv = sQ[ix[u] * kStTile + lane];
+                            if (e + u < e1) acc[j] = fma(nu[u], qv, acc[j]);
+                        }
+                    }
                 }
             }
             __syncthreads();
