@@ -221,17 +221,37 @@ __device__ __noinline__ float rate_of_progress_fp64(const DevMech& m, const DRxn
     }
 }
 
+// Ms = ctot + sum_e (eff_e - 1) C[sp_e] of reaction r (third_body.j2:18-31) in
+// FP32 at point `tid`, the efficiencies taken four at a time so that their
+// loads are in flight together; the sum keeps the table's order.
+__device__ __forceinline__ float tc_third_body(const DevMech& m, int r, const TileCtx& c, int tid) {
+    float Ms = c.ctot32;
+    const int e1 = __ldg(m.eff_ptr + r + 1);
+    for (int e = __ldg(m.eff_ptr + r); e < e1; e += 4) {
+        int sp[4];
+        float ev[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const bool ok = e + u < e1;
+            sp[u] = ok ? __ldg(m.eff_sp + e + u) : 0;
+            ev[u] = ok ? (float)__ldg(m.eff_val + e + u) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float cv = c.C[sp[u] * kTile + tid];
+            if (e + u < e1) Ms = fmaf(ev[u], cv, Ms);
+        }
+    }
+    return Ms;
+}
+
 // Net rate of progress of reaction r at point `tid` of the tile, FP32.
 __device__ float rate_of_progress(const DevMech& m, int r, const TileCtx& c, int tid) {
     const DRxn R = load_rxn(m.rxn + r);
     int kind = CG_STANDARD;
     while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
     float Ms = 0.0f;
-    if (kind >= CG_THIRD_BODY && kind <= CG_SRI) {
-        Ms = c.ctot32;
-        for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
-            Ms = fmaf((float)__ldg(m.eff_val + e), c.C[__ldg(m.eff_sp + e) * kTile + tid], Ms);
-    }
+    if (kind >= CG_THIRD_BODY && kind <= CG_SRI) Ms = tc_third_body(m, r, c, tid);
     const bool compact = (R.flags & kFCompact) != 0;
     const bool neg_falloff = kind >= CG_LINDEMANN && kind <= CG_SRI && (R.flags & (CG_F_A_NEG | CG_F_LOW_NEG));
     if (!compact || kind == CG_PLOG || neg_falloff) return rate_of_progress_fp64(m, R, kind, Ms, c, tid);
@@ -282,11 +302,7 @@ __device__ float rate_of_progress(const DevMech& m, int r, const TileCtx& c, int
 __device__ __forceinline__ float rate_fast(const DevMech& m, int r, const TcFast& F, const TileCtx& c, int tid) {
     const double a = fma(F.b, c.lnT2, F.l2A) - F.th2 * c.invT;
     float Ms = 1.0f;
-    if (F.flags & kFastThird) {
-        Ms = c.ctot32;
-        for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e)
-            Ms = fmaf((float)__ldg(m.eff_val + e), c.C[__ldg(m.eff_sp + e) * kTile + tid], Ms);
-    }
+    if (F.flags & kFastThird) Ms = tc_third_body(m, r, c, tid);
     const float cf = c.C[F.sr[0] * kTile + tid] * c.C[F.sr[1] * kTile + tid] * c.C[F.sr[2] * kTile + tid] * Ms;
     float q = rate32(a, cf, -32 * (int)F.ordf);
     if (F.flags & kFastRev) {
@@ -468,6 +484,8 @@ __global__ void __launch_bounds__(kTile * NT, 1)
                 float q = 0.0f;
                 if (r < m.nr) {
                     const TcFast F = load_fast(fast + r);
+                    // this thread's next record moves into L1 meanwhile (no registers held)
+                    if (u + 1 < kPer && r + 1 < m.nr) asm volatile("prefetch.global.L1 [%0];" ::"l"(fast + r + 1));
                     q = (F.flags & kFastOn) ? rate_fast(m, r, F, c, pt) : rate_of_progress(m, r, c, pt);
                 }
                 if (!act) q = 0.0f;
