@@ -18,7 +18,7 @@
 namespace cg {
 cudaError_t launch_getrates_fp64(const DevMech& m, const double* P, const double* T, const double* Y, double* wdot,
                                  int64_t ng, int block, double* scratch, int64_t scratch_blocks, cudaStream_t s);
-int fp64_smem_block(int ns, size_t smem_per_sm, size_t smem_per_block);
+int fp64_smem_block(int ns, size_t smem_per_sm, size_t smem_per_block, long* pts_per_sm);
 size_t fp64_global_slice_bytes(int ns);
 int fp64_global_blocks_per_sm();
 struct StagedPlan;
@@ -481,13 +481,19 @@ int chemgen_create(const void* blob, size_t nbytes, int device, chemgen_handle**
         return status_of(e);
     }
     h->sm_count = prop.multiProcessorCount;
-    h->fp64_block = cg::fp64_smem_block(h->ns, prop.sharedMemPerMultiprocessor, prop.sharedMemPerBlockOptin);
+    long smem_pts = 0;
+    h->fp64_block = cg::fp64_smem_block(h->ns, prop.sharedMemPerMultiprocessor, prop.sharedMemPerBlockOptin,
+                                        &smem_pts);
     h->fp64_slices = (int64_t)h->sm_count * cg::fp64_global_blocks_per_sm();
-    if (!h->fp64_block) {
-        // state too large for one thread per point in shared memory: the
-        // staged kernel when its tile fits, else the global-scratch kernel
+    // Fewer than 8 warps of points per SM in shared memory (state too large
+    // for one thread per point to hide its latencies): the staged kernel when
+    // its tile fits, else the global-scratch kernel (or the low-occupancy
+    // shared-memory kernel, when there is one)
+    if (!h->fp64_block || smem_pts < 256) {
         e = cg::staged_prepare(h->m, v, device, &h->staged);
-        if (e != cudaSuccess && e != cudaErrorNotSupported) {
+        if (e == cudaSuccess) {
+            h->fp64_block = 0;
+        } else if (e != cudaErrorNotSupported) {
             cudaFree(h->dbuf);
             delete h;
             return status_of(e);

@@ -750,7 +750,10 @@ static inline size_t point_bytes(int ns) { return (size_t)3 * ns * sizeof(double
 
 // Points per block for the shared-memory variant, chosen to maximise resident
 // points per SM; 0 when the state does not fit.
-int fp64_smem_block(int ns, size_t smem_per_sm, size_t smem_per_block) {
+// Block size (32, 64 or 128 points) of the one-thread-per-point kernel with
+// the most resident points per SM, or 0 when none fits; *pts_per_sm (may be
+// NULL) receives that number of points.
+int fp64_smem_block(int ns, size_t smem_per_sm, size_t smem_per_block, long* pts_per_sm) {
     int best_b = 0;
     long best_pts = 0;
     const int cands[3] = {32, 64, 128};
@@ -766,6 +769,7 @@ int fp64_smem_block(int ns, size_t smem_per_sm, size_t smem_per_block) {
             best_b = b;
         }
     }
+    if (pts_per_sm) *pts_per_sm = best_pts;
     return best_pts >= 64 ? best_b : 0;
 }
 
