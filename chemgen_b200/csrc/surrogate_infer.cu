@@ -16,14 +16,17 @@
 //   (cp.async.bulk, no multicast) brought into shared memory while the
 //   previous epilogue ran; epilogue l < 3: tcgen05.ld, bias, GELU (tanh form,
 //   hardware tanh as in training), BF16, into the A operand of the next layer
-//   (K = 256); epilogue l = 3: w_k = (u_k + b_k) exp(c + s (L + b_L)) in FP64,
-//   stored species-major, and the error estimate.  The compute group
-//   synchronises on its own named barrier.
+//   (K = 256), in two phases of 128 columns: between them the first half of
+//   the next layer's K is issued, into the other 256 tensor-memory columns,
+//   so that it runs beside the second phase; epilogue l = 3:
+//   w_k = (u_k + b_k) exp(c + s (L + b_L)) in FP64, stored species-major,
+//   and the error estimate.  The compute group synchronises on its own named
+//   barrier.
 // The weights come pre-arranged in the canonical layout (chemgen_surrogate_pack),
 // so every weight load is a straight 16-byte-aligned bulk copy.  Shared
 // memory: 64 KB activations + 32 KB features + 128 KB weights; tensor memory:
-// 256 columns; biases are read through the read-only cache.  Every mbarrier
-// wait is bounded; a time-out sets the error word and the kernel drains what
+// 512 columns (layer l accumulates in columns 256 (l % 2) ..); biases are
+// read through the read-only cache.  Every mbarrier wait is bounded; a time-out sets the error word and the kernel drains what
 // it issued before freeing tensor memory.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -188,9 +191,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     unsigned char* sA = sm;
     unsigned char* sF = sm + kFOff;
     unsigned char* sW = sm + kWOff;
-    // [0] MMAs done, [1] weights landed, [2] features full (128 arrivals), [3] features empty
+    // [0] MMAs done, [1] weights landed, [2] features full (128 arrivals), [3] features empty,
+    // [4] every product issued has completed (before tensor memory is freed)
     uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kTailOff);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 4);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 5);
     volatile int* wfail = reinterpret_cast<volatile int*>(tslot + 1);   // set by thread 0 before a barrier
     volatile int* mfail = wfail + 1;                                     // set after the MMA wait
     volatile int* ffail = wfail + 2;                                     // feature group gave up
@@ -206,12 +210,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         um::mbar_init(&bars[1], 1);
         um::mbar_init(&bars[2], kPts);
         um::mbar_init(&bars[3], 1);
+        um::mbar_init(&bars[4], 1);
         *wfail = 0;
         *mfail = 0;
         *ffail = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) um::tmem_alloc(tslot, 256);
+    if (warp == 0) um::tmem_alloc(tslot, 512);
     um::fence_before_sync();
     __syncthreads();
     um::fence_after_sync();
@@ -219,7 +224,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     float nrm[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) nrm[q] = __ldg(norm + q);
-    bool failed = false, w_pending = false, m_failed = false;
+    bool failed = false, w_pending = false;
     uint32_t mpar = 0, wpar = 0;
 
     if (tid >= kCompute) {
@@ -254,25 +259,45 @@ __global__ void __launch_bounds__(kThreads, 1)
             issue_weights(img, 0, sW, &bars[1]);
             w_pending = true;
         }
+        // Layer l accumulates in tensor-memory columns 256 (l % 2) .. + 255, so
+        // that the next layer's product can start before this layer's
+        // epilogue has read all of its accumulators: the epilogue of a hidden
+        // layer runs in two phases (columns 0-127, then 128-255), and between
+        // them thread 0 issues the first half of the next layer's K (which
+        // reads only activation columns 0-127); the second half follows the
+        // epilogue.
+        bool half_issued = false;     // thread 0: first K half of the next layer issued
         int j = 0;
         for (int64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x, ++j) {
             for (int l = 0; l < 4; ++l) {
                 const int K = layer_k(l), N = layer_n(l);
+                const uint32_t tacc = tbase + 256u * (uint32_t)(l & 1);
                 if (tid == 0) {
-                    const bool okw = um::mbar_wait(&bars[1], wpar);
-                    if (okw) {
-                        wpar ^= 1u;
-                        w_pending = false;
-                    }
-                    const bool okf = okw && (l != 0 || um::mbar_wait(&bars[2], (uint32_t)(j & 1)));
-                    if (okf) {
+                    const uint32_t idesc = um::idesc_bf16(kPts, N);
+                    if (l == 0) {
+                        const bool okw = um::mbar_wait(&bars[1], wpar);
+                        if (okw) {
+                            wpar ^= 1u;
+                            w_pending = false;
+                        }
+                        if (okw && um::mbar_wait(&bars[2], (uint32_t)(j & 1))) {
+                            um::fence_after_sync();
+                            const uint32_t a = um::smem_addr(sF), b = um::smem_addr(sW);
+                            for (int ks = 0; ks < K / 16; ++ks)
+                                um::mma_bf16(tacc, um::desc_kmajor(a, K, ks), um::desc_kmajor(b, K, ks), idesc,
+                                             ks > 0 ? 1u : 0u);
+                            um::commit(&bars[0]);
+                        } else {
+                            *wfail = 1;
+                        }
+                    } else if (half_issued) {
+                        // the second half of K: activation columns 128-255
                         um::fence_after_sync();
-                        const uint32_t idesc = um::idesc_bf16(kPts, N);
-                        const uint32_t a = um::smem_addr(l == 0 ? sF : sA), b = um::smem_addr(sW);
-                        for (int ks = 0; ks < K / 16; ++ks)
-                            um::mma_bf16(tbase, um::desc_kmajor(a, K, ks), um::desc_kmajor(b, K, ks), idesc,
-                                         ks > 0 ? 1u : 0u);
+                        const uint32_t a = um::smem_addr(sA), b = um::smem_addr(sW);
+                        for (int ks = K / 32; ks < K / 16; ++ks)
+                            um::mma_bf16(tacc, um::desc_kmajor(a, K, ks), um::desc_kmajor(b, K, ks), idesc, 1u);
                         um::commit(&bars[0]);
+                        half_issued = false;
                     } else {
                         *wfail = 1;
                     }
@@ -285,7 +310,6 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const bool ok = um::mbar_wait(&bars[0], mpar);
                 if (!ok) {
                     *mfail = 1;
-                    m_failed = true;
                 } else {
                     mpar ^= 1u;
                 }
@@ -303,13 +327,37 @@ __global__ void __launch_bounds__(kThreads, 1)
                     if (l < 3) {
                         const float* bl = bias + kHid * l;
 #pragma unroll 1
-                        for (int c = 128 * ehalf; c < 128 * ehalf + 128; c += 64) {
+                        for (int ph = 0; ph < 2; ++ph) {
+                            const int c = 128 * ph + 64 * ehalf;
                             uint32_t r[64];
-                            um::tmem_ld64(um::tmem_lane_addr(tbase, g4, c), r);
+                            um::tmem_ld64(um::tmem_lane_addr(tacc, g4, c), r);
 #pragma unroll
                             for (int q = 0; q < 4; ++q)
                                 gelu_store16(r + 16 * q, bl + c + 16 * q, sA + um::kmajor_offset(erow, c + 16 * q, kHid),
                                              sA + um::kmajor_offset(erow, c + 16 * q + 8, kHid));
+                            if (ph == 0) {
+                                // activation columns 0-127 are written: the next
+                                // layer's first K half can run beside phase 1
+                                um::fence_proxy_async();
+                                um::fence_before_sync();
+                                um::bar_sync(1, kCompute);
+                                if (tid == 0) {
+                                    const bool okw = um::mbar_wait(&bars[1], wpar);
+                                    if (okw) {
+                                        wpar ^= 1u;
+                                        w_pending = false;
+                                        um::fence_after_sync();
+                                        const int K2 = layer_k(l + 1);
+                                        const uint32_t idesc2 = um::idesc_bf16(kPts, layer_n(l + 1));
+                                        const uint32_t a = um::smem_addr(sA), b = um::smem_addr(sW);
+                                        const uint32_t t2 = tbase + 256u * (uint32_t)((l + 1) & 1);
+                                        for (int ks = 0; ks < K2 / 32; ++ks)
+                                            um::mma_bf16(t2, um::desc_kmajor(a, K2, ks), um::desc_kmajor(b, K2, ks),
+                                                         idesc2, ks > 0 ? 1u : 0u);
+                                        half_issued = true;
+                                    }
+                                }
+                            }
                         }
                     } else {
                         const float* b4 = bias + 3 * kHid;
@@ -318,7 +366,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         const bool oob = sOob[(j & 1) * kPts + erow] != 0;
                         const int cL = (ns / 16) * 16;
                         float v[16];
-                        um::tmem_ld16(um::tmem_lane_addr(tbase, g4, cL), v);
+                        um::tmem_ld16(um::tmem_lane_addr(tacc, g4, cL), v);
                         float L = 0.0f;
 #pragma unroll
                         for (int q = 0; q < 16; ++q)
@@ -326,7 +374,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         const double scale = exp(lc + ls * (double)(L + __ldg(b4 + ns)));
 #pragma unroll 1
                         for (int c = 32 * ehalf; c < 32 * ehalf + 32; c += 16) {
-                            um::tmem_ld16(um::tmem_lane_addr(tbase, g4, c), v);
+                            um::tmem_ld16(um::tmem_lane_addr(tacc, g4, c), v);
                             if (act) {
 #pragma unroll
                                 for (int q = 0; q < 16; ++q) {
@@ -337,6 +385,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                             }
                         }
                     }
+                } else if (l < 3) {
+                    um::bar_sync(1, kCompute);     // the mid-epilogue barrier the others reach
                 }
                 um::fence_proxy_async();
                 um::fence_before_sync();
@@ -349,19 +399,22 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             if (*ffail) failed = true;
         }
-        if (failed) {
-            // drain what this group issued (bounded) before tensor memory is freed
-            if (tid == 0) {
-                atomicExch(&g_sur_err, 1);
-                if (w_pending) um::mbar_wait(&bars[1], wpar);
-            }
-            if (m_failed) um::mbar_wait(&bars[0], mpar);
+        if (failed && tid == 0) {
+            // drain the weight copy this group issued (bounded)
+            atomicExch(&g_sur_err, 1);
+            if (w_pending) um::mbar_wait(&bars[1], wpar);
+        }
+        // every product issued (committed or not) completes before tensor
+        // memory is freed
+        if (tid == 0) {
+            um::commit(&bars[4]);
+            um::mbar_wait(&bars[4], 0);
         }
     }
     if (tid >= kCompute && *ffail && tid == kCompute) atomicExch(&g_sur_err, 1);
     um::fence_before_sync();
     __syncthreads();
-    if (warp == 0) um::tmem_dealloc(tbase, 256);
+    if (warp == 0) um::tmem_dealloc(tbase, 512);
 }
 
 // Weight image: layer l's [N_l x K_l] BF16 operand in the K-major canonical
