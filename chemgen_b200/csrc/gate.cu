@@ -14,7 +14,9 @@
 //   held, which the caller keeps a valid state.
 // * gate_scatter: W[k*ng + idx[j]] = Wc[k*cap + j] for j < min(*count, cap).
 // All three are grid-stride loops over a device-side count, so a launch has
-// the same shape whatever the count is.
+// the same shape whatever the count is; gather and scatter give each thread
+// one (species, slot) pair, so a few thousand points still spread over
+// hundreds of thousands of independent loads.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -26,21 +28,32 @@ namespace {
 __global__ void gate_select_kernel(const float* __restrict__ est, float thr, int64_t ng, int64_t* __restrict__ idx,
                                    int64_t cap, unsigned long long* __restrict__ count) {
     const int lane = threadIdx.x & 31;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    // the trip count is the same for every lane of a warp (blockDim is a
-    // multiple of 32), so the ballot below always has the full warp
-    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < ng; base += stride) {
-        const int64_t i = base + threadIdx.x;
-        const bool bad = i < ng && !(__ldcs(est + i) <= thr);
-        const unsigned m = __ballot_sync(0xffffffffu, bad);
-        if (m == 0u) continue;
-        const int leader = __ffs(m) - 1;
-        unsigned long long b0 = 0;
-        if (lane == leader) b0 = atomicAdd(count, (unsigned long long)__popc(m));
-        b0 = __shfl_sync(0xffffffffu, b0, leader);
-        if (bad) {
-            const int64_t slot = (int64_t)b0 + __popc(m & ((1u << lane) - 1u));
-            if (slot < cap) idx[slot] = i;
+    const int64_t step = (int64_t)blockDim.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x * 4;
+    // four estimates per thread in flight at once; the trip count is the
+    // same for every lane of a warp (blockDim is a multiple of 32), so the
+    // ballots below always have the full warp
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x * 4; base < ng; base += stride) {
+        float e[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t i = base + u * step + threadIdx.x;
+            e[u] = i < ng ? __ldcs(est + i) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t i = base + u * step + threadIdx.x;
+            const bool bad = i < ng && !(e[u] <= thr);
+            const unsigned m = __ballot_sync(0xffffffffu, bad);
+            if (m == 0u) continue;
+            const int leader = __ffs(m) - 1;
+            unsigned long long b0 = 0;
+            if (lane == leader) b0 = atomicAdd(count, (unsigned long long)__popc(m));
+            b0 = __shfl_sync(0xffffffffu, b0, leader);
+            if (bad) {
+                const int64_t slot = (int64_t)b0 + __popc(m & ((1u << lane) - 1u));
+                if (slot < cap) idx[slot] = i;
+            }
         }
     }
 }
@@ -50,30 +63,36 @@ __device__ __forceinline__ int64_t active_slots(const unsigned long long* count,
     return n < cap ? n : cap;
 }
 
+// One thread per (row, slot) pair, slots fastest: rows 0..ns-1 are the
+// species, row ns is P and row ns+1 is T; the batch side is coalesced.
 __global__ void gate_gather_kernel(const double* __restrict__ P, const double* __restrict__ T,
                                    const double* __restrict__ Y, int ns, int64_t ng, const int64_t* __restrict__ idx,
                                    const unsigned long long* __restrict__ count, int64_t cap, double* __restrict__ Pc,
                                    double* __restrict__ Tc, double* __restrict__ Yc) {
     const int64_t n = active_slots(count, cap);
+    const int64_t total = n * (ns + 2);
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        const int k = (int)(t / n);
+        const int64_t j = t - (int64_t)k * n;
         const int64_t i = idx[j];
-        Pc[j] = P[i];
-        Tc[j] = T[i];
-#pragma unroll 8
-        for (int k = 0; k < ns; ++k) Yc[(int64_t)k * cap + j] = Y[(int64_t)k * ng + i];
+        if (k < ns) Yc[(int64_t)k * cap + j] = Y[(int64_t)k * ng + i];
+        else if (k == ns) Pc[j] = P[i];
+        else Tc[j] = T[i];
     }
 }
 
+// One thread per (species, slot) pair, slots fastest.
 __global__ void gate_scatter_kernel(const double* __restrict__ Wc, int ns, int64_t cap,
                                     const int64_t* __restrict__ idx, const unsigned long long* __restrict__ count,
                                     double* __restrict__ W, int64_t ng) {
     const int64_t n = active_slots(count, cap);
+    const int64_t total = n * ns;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
-        const int64_t i = idx[j];
-#pragma unroll 8
-        for (int k = 0; k < ns; ++k) W[(int64_t)k * ng + i] = Wc[(int64_t)k * cap + j];
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        const int k = (int)(t / n);
+        const int64_t j = t - (int64_t)k * n;
+        W[(int64_t)k * ng + idx[j]] = Wc[(int64_t)k * cap + j];
     }
 }
 
@@ -105,7 +124,7 @@ int chemgen_gate_select(const float* est, float thr, int64_t ng, int64_t* idx, i
     cudaStream_t s = (cudaStream_t)stream;
     if (cudaMemsetAsync(count, 0, sizeof(uint64_t), s) != cudaSuccess) return CHEMGEN_ERR_CUDA;
     if (ng == 0) return CHEMGEN_OK;
-    gate_select_kernel<<<grid_for(ng, 8), 256, 0, s>>>(est, thr, ng, idx, cap,
+    gate_select_kernel<<<grid_for((ng + 3) / 4, 8), 256, 0, s>>>(est, thr, ng, idx, cap,
                                                         reinterpret_cast<unsigned long long*>(count));
     return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA;
 }
@@ -118,7 +137,7 @@ int chemgen_gate_gather(const double* P, const double* T, const double* Y, int n
                           (const void*)Pc, (const void*)Tc, (const void*)Yc})
         if (!aligned8(p)) return CHEMGEN_ERR_MISALIGNED;
     if (ng == 0 || cap == 0) return CHEMGEN_OK;
-    gate_gather_kernel<<<grid_for(cap, 2), 256, 0, (cudaStream_t)stream>>>(
+    gate_gather_kernel<<<grid_for(cap * (ns + 2), 4), 256, 0, (cudaStream_t)stream>>>(
         P, T, Y, ns, ng, idx, reinterpret_cast<const unsigned long long*>(count), cap, Pc, Tc, Yc);
     return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA;
 }
@@ -129,7 +148,7 @@ int chemgen_gate_scatter(const double* Wc, int ns, int64_t cap, const int64_t* i
     for (const void* p : {(const void*)Wc, (const void*)idx, (const void*)count, (const void*)W})
         if (!aligned8(p)) return CHEMGEN_ERR_MISALIGNED;
     if (ng == 0 || cap == 0) return CHEMGEN_OK;
-    gate_scatter_kernel<<<grid_for(cap, 2), 256, 0, (cudaStream_t)stream>>>(
+    gate_scatter_kernel<<<grid_for(cap * ns, 4), 256, 0, (cudaStream_t)stream>>>(
         Wc, ns, cap, idx, reinterpret_cast<const unsigned long long*>(count), W, ng);
     return cudaGetLastError() == cudaSuccess ? CHEMGEN_OK : CHEMGEN_ERR_CUDA;
 }

@@ -26,8 +26,9 @@
 // so every weight load is a straight 16-byte-aligned bulk copy.  Shared
 // memory: 64 KB activations + 32 KB features + 128 KB weights; tensor memory:
 // 512 columns (layer l accumulates in columns 256 (l % 2) ..); biases are
-// read through the read-only cache.  Every mbarrier wait is bounded; a time-out sets the error word and the kernel drains what
-// it issued before freeing tensor memory.
+// read through the read-only cache.  Every mbarrier wait is bounded; a
+// time-out sets the error word, and the kernel waits for every product it
+// issued before freeing tensor memory.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 

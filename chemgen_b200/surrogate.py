@@ -773,7 +773,9 @@ class SurrogateGetrates:
     def _buffers(self, ng: int):
         """Batch buffers of the device gate; the unused slots always hold a
         valid state (1 atm, 1000 K, equal mass fractions, or a state of an
-        earlier call), so the exact kernel's work on them is harmless."""
+        earlier call), so the exact kernel's work on them is harmless.  The
+        error-estimate buffer follows ng; device pointers are kept so that a
+        call does little host work between its launches."""
         import torch
         cap = min(ng, max(self._cap, self.MIN_CAP))
         b = self._bufs
@@ -786,29 +788,40 @@ class SurrogateGetrates:
                  "idx": torch.empty(cap, dtype=torch.int64, device=dev),
                  "count": torch.zeros(1, dtype=torch.int64, device=dev),
                  "count_host": torch.zeros(1, dtype=torch.int64, pin_memory=True),
-                 "done": torch.cuda.Event()}
+                 "done": torch.cuda.Event(), "est": None}
+            for k in ("P", "T", "Y", "W", "idx", "count"):
+                b["p_" + k] = b[k].data_ptr()
             self._bufs = b
+        if b["est"] is None or b["est"].numel() != ng:
+            b["est"] = torch.empty(ng, dtype=torch.float32, device=self.sur.dev)
         return b
 
-    def __call__(self, P, T, Y):
+    def __call__(self, P, T, Y, out=None):
+        """wdot [ns, ng] (FP64, species-major) for P[ng], T[ng], Y[ns, ng];
+        written into `out` when given."""
         import torch
         P, T, Y = P.contiguous(), T.contiguous(), Y.contiguous()
-        # the fused kernel folds the training-support check into the estimate
-        W, est = self.sur.predict(P, T, Y, check_range=True)
         ng = T.numel()
-        if not (W.is_cuda and ng):
+        if not (T.is_cuda and ng):
+            # the fused kernel folds the training-support check into the estimate
+            W, est = self.sur.predict(P, T, Y, check_range=True)
             self.last_fallback = self._host_gate(P, T, Y, W, est) / max(ng, 1)
+            if out is not None:
+                out.copy_(W)
+                return out
             return W
         b = self._buffers(ng)
-        cap, ns, s = b["cap"], self.sur.ns, _stream()
-        check(lib().chemgen_gate_select(est.data_ptr(), self.threshold, ng, b["idx"].data_ptr(), cap,
-                                        b["count"].data_ptr(), s), "gate_select")
-        check(lib().chemgen_gate_gather(P.data_ptr(), T.data_ptr(), Y.data_ptr(), ns, ng, b["idx"].data_ptr(),
-                                        b["count"].data_ptr(), cap, b["P"].data_ptr(), b["T"].data_ptr(),
-                                        b["Y"].data_ptr(), s), "gate_gather")
-        self.sur.gm.getrates(b["P"], b["T"], b["Y"], out=b["W"], mode=self.exact_mode)
-        check(lib().chemgen_gate_scatter(b["W"].data_ptr(), ns, cap, b["idx"].data_ptr(), b["count"].data_ptr(),
-                                         W.data_ptr(), ng, s), "gate_scatter")
+        est = b["est"]
+        W = out if out is not None else torch.empty((self.sur.ns, ng), dtype=torch.float64, device=self.sur.dev)
+        self.sur.predict_fused(P, T, Y, W, est, check_range=True)
+        cap, ns, s, L = b["cap"], self.sur.ns, _stream(), lib()
+        check(L.chemgen_gate_select(est.data_ptr(), self.threshold, ng, b["p_idx"], cap, b["p_count"], s),
+              "gate_select")
+        check(L.chemgen_gate_gather(P.data_ptr(), T.data_ptr(), Y.data_ptr(), ns, ng, b["p_idx"], b["p_count"], cap,
+                                    b["p_P"], b["p_T"], b["p_Y"], s), "gate_gather")
+        self.sur.gm.getrates_ptr(b["p_P"], b["p_T"], cap, b["p_Y"], b["p_W"], self.exact_mode, s)
+        check(L.chemgen_gate_scatter(b["p_W"], ns, cap, b["p_idx"], b["p_count"], W.data_ptr(), ng, s),
+              "gate_scatter")
         b["count_host"].copy_(b["count"], non_blocking=True)
         b["done"].record()
         b["done"].synchronize()
