@@ -631,6 +631,154 @@ __global__ void __launch_bounds__(32 * kJMaxWarps, 1)
     }
 }
 
+// ------------------------------------------------ tile VJP kernel
+//
+// dL/d(T, Y, P) from the cotangent G = dL/dwdot without J and without global
+// scratch.  A persistent CTA owns a tile of 32 points (one per lane) and keeps
+// the tile's C, EGp, dEGp/dT and G in shared memory.  Warp w evaluates the
+// rate derivatives of reactions w, w + W, ... and adds their contributions
+// into dL/dC accumulators [ns][32] of its own (shared memory, no atomics); at
+// the end of the tile the W copies are added in warp order, so the result
+// does not depend on scheduling.  The chain rule through C(T, Y) then follows
+// the in-place kernel's (file header).
+constexpr int kVMaxWarps = 16;
+
+__global__ void __launch_bounds__(32 * kVMaxWarps, 1)
+    vjp_tile_kernel(DevMech m, const double* __restrict__ P, const double* __restrict__ Tg,
+                    const double* __restrict__ Y, const double* __restrict__ G, double* __restrict__ gT,
+                    double* __restrict__ gY, double* __restrict__ gP, int64_t ng) {
+    extern __shared__ double smem[];
+    const int ns = m.ns;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double* sC = smem;
+    double* sE = sC + ns * kJTile;
+    double* sD = sE + ns * kJTile;
+    double* sG = sD + ns * kJTile;
+    double* sRed = sG + ns * kJTile;                                   // [3][kVMaxWarps][32]
+    double* sAcc = sRed + 3 * kVMaxWarps * kJTile;                     // [nw][ns][32]
+    double* acc = sAcc + (size_t)warp * ns * kJTile + lane;            // this warp's dL/dC
+    const int64_t ntiles = (ng + kJTile - 1) / kJTile;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int64_t i = tile * kJTile + lane;
+        const bool act = i < ng;
+        const double T = act ? Tg[i] : 1000.0;
+        const double Pv = act ? P[i] : kPatm;
+        PointT pt;
+        pt.T = T;
+        pt.lnT = cgm::cg_log(T);
+        pt.invT = 1.0 / T;
+        double part = 0.0;
+        for (int k = warp; k < ns; k += nw) {
+            const double c = (act ? Y[(int64_t)k * ng + i] : 1.0) * __ldg(m.inv_mw + k);
+            sC[k * kJTile + lane] = c;
+            sG[k * kJTile + lane] = act ? G[(int64_t)k * ng + i] : 0.0;
+            part += c;
+        }
+        for (int k = 0; k < ns; ++k) acc[k * kJTile] = 0.0;
+        sRed[warp * kJTile + lane] = part;
+        __syncthreads();
+        double S = 0.0;
+        for (int w = 0; w < nw; ++w) S += sRed[w * kJTile + lane];
+        const double fac = Pv / (kR0 * S * T);
+        const double pfac = kPatm / (kR0 * T);
+        part = 0.0;
+        for (int k = warp; k < ns; k += nw) {
+            const double c = sC[k * kJTile + lane] * fac;
+            sC[k * kJTile + lane] = c;
+            part += c;
+            const double* th = m.thermo + 16 * k;
+            const double* cf = (T < __ldg(th)) ? th + 1 : th + 8;
+            double cc[7];
+#pragma unroll
+            for (int j = 0; j < 7; ++j) cc[j] = __ldg(cf + j);
+            sE[k * kJTile + lane] = cgm::cg_exp_clamped(smh_poly(cc, T, pt.lnT, pt.invT)) * pfac;
+            const double dp = fma(fma(fma(4.0 * cc[5], T, 3.0 * cc[4]), T, 2.0 * cc[3]), T, cc[2]);
+            sD[k * kJTile + lane] = dp + fma(cc[6], pt.invT, cc[1]) * pt.invT - pt.invT;
+        }
+        __syncthreads();                     // S read by every warp before sRed is reused
+        sRed[warp * kJTile + lane] = part;
+        __syncthreads();
+        double ctot = 0.0;
+        for (int w = 0; w < nw; ++w) ctot += sRed[w * kJTile + lane];
+        const double lnP = cgm::cg_log(Pv);
+        const DState st{sC + lane, sE + lane, sD + lane, nullptr, kJTile};
+        const double* Gl = sG + lane;
+        double tb = 0.0, ab = 0.0, pb = 0.0;
+        for (int r = warp; r < m.nr; r += nw) {
+            const DRxn R = load_rxn(m.rxn + r);
+            double gq = 0.0, dqdT, dqdM, plog_term = 0.0;
+            bool usesM;
+            if (R.flags & kFCompact) {
+                SideT<3> re, pr;
+                RxnGradT<3> g;
+                reaction_grad<3>(m, r, R, pt, ctot, Pv, lnP, st, re, pr, g);
+                for (int j = 0; j < re.n; ++j) gq = fma(-re.nu[j], Gl[re.sp[j] * kJTile], gq);
+                for (int j = 0; j < pr.n; ++j) gq = fma(pr.nu[j], Gl[pr.sp[j] * kJTile], gq);
+                for (int j = 0; j < g.nd; ++j) acc[g.dsp[j] * kJTile] = fma(gq, g.dqc[j], acc[g.dsp[j] * kJTile]);
+                dqdT = g.dqdT;
+                dqdM = g.dqdM;
+                usesM = g.usesM;
+                if (g.kind == CG_PLOG) plog_term = g.qnet * g.dlkf_lnP / Pv;
+            } else {
+                Side re, pr;
+                RxnGrad g;
+                reaction_grad<16>(m, r, R, pt, ctot, Pv, lnP, st, re, pr, g);
+                for (int j = 0; j < re.n; ++j) gq = fma(-re.nu[j], Gl[re.sp[j] * kJTile], gq);
+                for (int j = 0; j < pr.n; ++j) gq = fma(pr.nu[j], Gl[pr.sp[j] * kJTile], gq);
+                for (int j = 0; j < g.nd; ++j) acc[g.dsp[j] * kJTile] = fma(gq, g.dqc[j], acc[g.dsp[j] * kJTile]);
+                dqdT = g.dqdT;
+                dqdM = g.dqdM;
+                usesM = g.usesM;
+                if (g.kind == CG_PLOG) plog_term = g.qnet * g.dlkf_lnP / Pv;
+            }
+            tb = fma(gq, dqdT, tb);
+            if (usesM) {
+                ab = fma(gq, dqdM, ab);
+                for (int e = __ldg(m.eff_ptr + r); e < __ldg(m.eff_ptr + r + 1); ++e) {
+                    double* o = acc + __ldg(m.eff_sp + e) * kJTile;
+                    *o = fma(gq * dqdM, __ldg(m.eff_val + e), *o);
+                }
+            }
+            pb = fma(gq, plog_term, pb);
+        }
+        sRed[warp * kJTile + lane] = tb;
+        sRed[(kVMaxWarps + warp) * kJTile + lane] = ab;
+        sRed[(2 * kVMaxWarps + warp) * kJTile + lane] = pb;
+        __syncthreads();
+        tb = ab = pb = 0.0;
+        for (int w = 0; w < nw; ++w) {
+            tb += sRed[w * kJTile + lane];
+            ab += sRed[(kVMaxWarps + w) * kJTile + lane];
+            pb += sRed[(2 * kVMaxWarps + w) * kJTile + lane];
+        }
+        // dL/dC_k = sum over the warps' copies (in warp order) + dL/dM; this
+        // warp's species' share of rho = sum_k dL/dC_k C_k
+        double rpart = 0.0;
+        for (int k = warp; k < ns; k += nw) {
+            double cb = 0.0;
+            for (int w = 0; w < nw; ++w) cb += sAcc[((size_t)w * ns + k) * kJTile + lane];
+            cb += ab;
+            sG[k * kJTile + lane] = cb;          // G is no longer needed
+            rpart = fma(cb, sC[k * kJTile + lane], rpart);
+        }
+        __syncthreads();                     // tb, ab, pb read before sRed is reused
+        sRed[warp * kJTile + lane] = rpart;
+        __syncthreads();
+        double rho = 0.0;
+        for (int w = 0; w < nw; ++w) rho += sRed[w * kJTile + lane];
+        const double iS = 1.0 / S;
+        if (act) {
+            for (int k = warp; k < ns; k += nw)
+                gY[(int64_t)k * ng + i] = fma(ctot, sG[k * kJTile + lane], -rho) * __ldg(m.inv_mw + k) * iS;
+            if (warp == 0) {
+                gT[i] = tb - rho * pt.invT;
+                if (gP) gP[i] = fma(rho, 1.0 / Pv, pb);
+            }
+        }
+        __syncthreads();                     // the tile's state stays until every warp is done
+    }
+}
+
 }  // namespace
 
 // Row-owner Jacobian plan: per-species (reaction, net nu) lists.
@@ -759,9 +907,33 @@ cudaError_t launch_jacobian(const DevMech& m, int precision, const double* P, co
     return cudaGetLastError();
 }
 
+// Warps per CTA of the tile VJP kernel for ns species (its shared memory
+// holds 4 + W arrays of [ns][32] doubles), or 0 when fewer than 4 fit.
+int vjp_tile_warps(int ns, size_t smem_optin) {
+    const size_t arr = (size_t)ns * kJTile * 8, fixed = 4 * arr + (size_t)3 * kVMaxWarps * kJTile * 8;
+    if (fixed + 4 * arr > smem_optin) return 0;
+    const size_t w = (smem_optin - fixed) / arr;
+    return (int)std::min<size_t>(w, kVMaxWarps);
+}
+
 cudaError_t launch_vjp(const DevMech& m, const double* P, const double* T, const double* Y, const double* G, double* gT,
                        double* gY, double* gP, int64_t ng, double* scratch, int sm_count, cudaStream_t s) {
     if (ng <= 0) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    int optin = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    const int w = vjp_tile_warps(m.ns, (size_t)optin);
+    if (w >= 4) {
+        const size_t smem = (size_t)(4 + w) * m.ns * kJTile * 8 + (size_t)3 * kVMaxWarps * kJTile * 8;
+        e = cudaFuncSetAttribute(vjp_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        const int64_t tiles = (ng + kJTile - 1) / kJTile;
+        const unsigned grid = (unsigned)std::min<int64_t>(tiles, sm_count);
+        vjp_tile_kernel<<<grid, 32u * (unsigned)w, smem, s>>>(m, P, T, Y, G, gT, gY, gP, ng);
+        return cudaGetLastError();
+    }
     int64_t blocks = (ng + 127) / 128;
     if (blocks > (int64_t)sm_count * 16) blocks = (int64_t)sm_count * 16;
     deriv_kernel<false, double><<<(unsigned)blocks, 128, 0, s>>>(m, P, T, Y, G, nullptr, gT, gY, gP, scratch, ng);

@@ -169,6 +169,33 @@ def test_vjp_equals_jacobian_transpose_and_autograd_function():
     assert torch.allclose(Tr.grad, gT) and torch.allclose(Yr.grad, gY)
 
 
+@pytest.mark.parametrize("name,ng", [("gri30", 32 * 70 + 5), ("synthetic_53_325", 65536)])
+def test_vjp_53_species_matches_jacobian_transpose(name, ng):
+    """The C4 mechanisms on the tile adjoint kernel (shared-memory state,
+    per-warp accumulators added in a fixed order), ragged last tile included:
+    the VJP equals J^T G from the row-owner Jacobian, and two calls agree bit
+    for bit."""
+    import torch
+    mech, d = load_golden(name)
+    blob = pack.pack(mech).to_blob()
+    P, T, Y = synthetic.states(mech.ns, ng, seed=21)
+    gm = GpuMechanism(blob)
+    Pt, Tt, Yt = _t(P), _t(T), _t(Y)
+    G = torch.randn(mech.ns, ng, dtype=torch.float64, device="cuda",
+                    generator=torch.Generator(device="cuda").manual_seed(5))
+    J = gm.jacobian(Pt, Tt, Yt)
+    gT, gY, gP = gm.vjp(Pt, Tt, Yt, G)
+    gT2, gY2, gP2 = gm.vjp(Pt, Tt, Yt, G)
+    assert torch.equal(gT, gT2) and torch.equal(gY, gY2) and torch.equal(gP, gP2)
+    ref_T = (J[:, 0, :] * G).sum(0)
+    ref_Y = torch.einsum("kjn,kn->jn", J[:, 1:, :], G)
+    # per point, relative to that point's largest term
+    eT = ((gT - ref_T).abs() / (J[:, 0, :].abs() * G.abs()).sum(0).clamp_min(1e-300)).max().item()
+    eY = ((gY - ref_Y).abs().max(0).values /
+          torch.einsum("kjn,kn->jn", J[:, 1:, :].abs(), G.abs()).max(0).values.clamp_min(1e-300)).max().item()
+    assert eT < 1e-10 and eY < 1e-10, (eT, eY)
+
+
 def test_jacobian_with_zero_species_is_exact():
     """Y_j = 0 exactly: the analytic derivative must not vanish where FD says it doesn't."""
     import torch
