@@ -234,7 +234,10 @@ using RxnGrad = RxnGradT<16>;
 // kb, and for three-body and falloff reactions M and d ln kf/dM (gM).  The
 // row-owner Jacobian computes them once per reaction and tile (KC = 5
 // values, stride 32 apart, in `kc`); reaction_grad can take them from there.
-constexpr int kKC = 5;   // kf, kb, dlkf, gM, M
+// per-reaction slots of the row-owner kernel's tile cache: a compact
+// reaction's derivatives (dq/dT, dq/dM, dq/dC of its six slots), or another
+// reaction's five rate constants (kf, kb, dlkf, gM, M)
+constexpr int kDC = 8;
 
 __device__ __forceinline__ void reaction_k(const DevMech& m, int r, const DRxn& R, int kind, const PointT& pt,
                                            double ctot, double Pv, double lnP, const DState& st, double& kf,
@@ -557,16 +560,28 @@ __global__ void __launch_bounds__(32 * kJMaxWarps, 1)
         const double lnP = cgm::cg_log(Pv);
         const DState st{sC + lane, sE + lane, sD + lane, nullptr, kJTile};
         const double iS = 1.0 / S;
-        // phase 1: every reaction's rate constants once, into this CTA's
-        // slice [nr][kKC][32] (a few hundred KB: it stays in L2)
-        double* kc = kcache + (int64_t)blockIdx.x * m.nr * kKC * kJTile;
+        // phase 1: every reaction once, into this CTA's slice [nr][kDC][32]
+        // (a few hundred KB: it stays in L2): a compact reaction's rate
+        // derivatives, which the rows then only gather, or another reaction's
+        // rate constants, from which each row that needs it evaluates them
+        double* kc = kcache + (int64_t)blockIdx.x * m.nr * kDC * kJTile;
         for (int r = warp; r < m.nr; r += nw) {
             const DRxn R = load_rxn(m.rxn + r);
+            double* o = kc + (int64_t)r * kDC * kJTile + lane;
+            if (R.flags & kFCompact) {
+                SideT<3> re, pr;
+                RxnGradT<3> g;
+                reaction_grad<3>(m, r, R, pt, ctot, Pv, lnP, st, re, pr, g);
+                o[0] = g.dqdT;
+                o[32] = g.dqdM;
+#pragma unroll
+                for (int j = 0; j < 6; ++j) o[(2 + j) * kJTile] = g.dqc[j];
+                continue;
+            }
             int kind = CG_STANDARD;
             while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
             double kf, kb, dlkf, gM, M, dlp;
             reaction_k(m, r, R, kind, pt, ctot, Pv, lnP, st, kf, kb, dlkf, gM, M, dlp);
-            double* o = kc + (int64_t)r * kKC * kJTile + lane;
             o[0] = kf;
             o[32] = kb;
             o[64] = dlkf;
@@ -584,16 +599,29 @@ __global__ void __launch_bounds__(32 * kJMaxWarps, 1)
                 const DRxn R = load_rxn(m.rxn + r);
                 double dqdT, dqdM;
                 bool usesM;
-                const double* kr = kc + (int64_t)r * kKC * kJTile + lane;
+                const double* kr = kc + (int64_t)r * kDC * kJTile + lane;
                 if (R.flags & kFCompact) {
+                    // the derivatives from phase 1; the slots' species as
+                    // reaction_grad<3> lays them out
                     SideT<3> re, pr;
-                    RxnGradT<3> g;
-                    reaction_grad<3, true>(m, r, R, pt, ctot, Pv, lnP, st, re, pr, g, kr);
+                    load_sides3(R, re, pr);
+                    const bool rev = (R.flags & CG_F_REVERSIBLE) != 0;
+                    int dsp[6];
 #pragma unroll
-                    for (int j = 0; j < 6; ++j) row[(1 + g.dsp[j]) * kJTile] = fma(nu, g.dqc[j], row[(1 + g.dsp[j]) * kJTile]);
-                    dqdT = g.dqdT;
-                    dqdM = g.dqdM;
-                    usesM = g.usesM;
+                    for (int j = 0; j < 3; ++j) {
+                        dsp[j] = j < re.n ? re.sp[j] : 0;
+                        dsp[3 + j] = (rev && j < pr.n) ? pr.sp[j] : 0;
+                    }
+                    double dq[6];
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) dq[j] = kr[(2 + j) * kJTile];
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) row[(1 + dsp[j]) * kJTile] = fma(nu, dq[j], row[(1 + dsp[j]) * kJTile]);
+                    dqdT = kr[0];
+                    dqdM = kr[32];
+                    int kind = CG_STANDARD;
+                    while (kind < CG_PLOG && r >= m.seg[kind + 1]) ++kind;
+                    usesM = kind >= CG_THIRD_BODY && kind <= CG_SRI;
                 } else {
                     Side re, pr;
                     RxnGrad g;
@@ -871,7 +899,7 @@ void jac_release(JacPlan* p) {
 size_t jac_rows_workspace_bytes(const JacPlan* p, const DevMech& m, int64_t ng) {
     const int64_t tiles = (ng + kJTile - 1) / kJTile;
     const int64_t grid = std::min<int64_t>(tiles, p->grid);
-    return (size_t)grid * m.nr * kKC * kJTile * sizeof(double);
+    return (size_t)grid * m.nr * kDC * kJTile * sizeof(double);
 }
 
 cudaError_t launch_jacobian_rows(const JacPlan* p, const DevMech& m, int precision, const double* P, const double* T,
