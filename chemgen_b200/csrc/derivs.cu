@@ -506,7 +506,8 @@ constexpr int kJMaxWarps = 8;
 template <typename JT>
 __global__ void __launch_bounds__(32 * kJMaxWarps, 1)
     jac_rows_kernel(DevMech m, const int* __restrict__ lptr, const int* __restrict__ lrx,
-                    const double* __restrict__ lnu, const double* __restrict__ P, const double* __restrict__ Tg,
+                    const double* __restrict__ lnu, const int* __restrict__ lrow, const double* __restrict__ P,
+                    const double* __restrict__ Tg,
                     const double* __restrict__ Y, JT* __restrict__ J, int64_t ng, double* __restrict__ kcache) {
     extern __shared__ double smem[];
     const int ns = m.ns, ncol = ns + 1;
@@ -589,7 +590,10 @@ __global__ void __launch_bounds__(32 * kJMaxWarps, 1)
             o[128] = M;
         }
         __syncthreads();
-        for (int k = warp; k < ns; k += nw) {
+        // rows t = warp, warp + nw, ...: species lrow[t], dealt out so that the
+        // warps' lists are about equally long and reach the barrier together
+        for (int t = warp; t < ns; t += nw) {
+            const int k = __ldg(lrow + t);
             for (int c = 0; c < ncol; ++c) row[c * kJTile] = 0.0;
             double ak = 0.0;
             const int e1 = __ldg(lptr + k + 1);
@@ -817,6 +821,7 @@ struct JacPlan {
     const int* lptr = nullptr;
     const int* lrx = nullptr;
     const double* lnu = nullptr;
+    const int* lrow = nullptr;  // species of row slot t (warp t % warps)
     void* dbuf = nullptr;
 };
 
@@ -861,19 +866,42 @@ cudaError_t jac_prepare(const DevMech& m, const cg_mech_view& v, int device, Jac
         }
         lptr[k + 1] = (int)lrx.size();
     }
+    // row slots: warp w takes slots w, w + warps, ...; species dealt out
+    // longest list first, each to the warp with the least work so far among
+    // those with a free slot (a row costs its list plus the chain rule)
+    std::vector<int> order(ns);
+    for (int k = 0; k < ns; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return lists[a].size() > lists[b].size(); });
+    std::vector<std::vector<int>> warp_rows(warps);
+    std::vector<long> load(warps, 0);
+    for (int k : order) {
+        int best = -1;
+        for (int w = 0; w < warps; ++w) {
+            const int cap = (ns - w + warps - 1) / warps;
+            if ((int)warp_rows[w].size() < cap && (best < 0 || load[w] < load[best])) best = w;
+        }
+        warp_rows[best].push_back(k);
+        load[best] += (long)lists[k].size() + ns;
+    }
+    std::vector<int> lrow(ns);
+    for (int w = 0; w < warps; ++w)
+        for (size_t j = 0; j < warp_rows[w].size(); ++j) lrow[j * warps + w] = warp_rows[w][j];
     const size_t b_ptr = ((ns + 1) * sizeof(int) + 255) / 256 * 256;
     const size_t b_rx = (std::max<size_t>(lrx.size(), 1) * sizeof(int) + 255) / 256 * 256;
-    const size_t b_nu = std::max<size_t>(lnu.size(), 1) * sizeof(double);
+    const size_t b_nu = (std::max<size_t>(lnu.size(), 1) * sizeof(double) + 255) / 256 * 256;
+    const size_t b_row = (size_t)ns * sizeof(int);
     JacPlan* p = new JacPlan();
     p->warps = warps;
     p->smem = fixed + (size_t)warps * per_warp;
     p->grid = prop.multiProcessorCount;
-    e = cudaMalloc(&p->dbuf, b_ptr + b_rx + b_nu);
+    e = cudaMalloc(&p->dbuf, b_ptr + b_rx + b_nu + b_row);
     char* d = (char*)p->dbuf;
     if (e == cudaSuccess) e = cudaMemcpy(d, lptr.data(), lptr.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !lrx.empty()) e = cudaMemcpy(d + b_ptr, lrx.data(), lrx.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !lnu.empty())
         e = cudaMemcpy(d + b_ptr + b_rx, lnu.data(), lnu.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d + b_ptr + b_rx + b_nu, lrow.data(), b_row, cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(jac_rows_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem);
     if (e == cudaSuccess)
@@ -886,6 +914,7 @@ cudaError_t jac_prepare(const DevMech& m, const cg_mech_view& v, int device, Jac
     p->lptr = (const int*)d;
     p->lrx = (const int*)(d + b_ptr);
     p->lnu = (const double*)(d + b_ptr + b_rx);
+    p->lrow = (const int*)(d + b_ptr + b_rx + b_nu);
     *out = p;
     return cudaSuccess;
 }
@@ -911,11 +940,11 @@ cudaError_t launch_jacobian_rows(const JacPlan* p, const DevMech& m, int precisi
     if (!scratch || scratch_bytes < jac_rows_workspace_bytes(p, m, ng)) return cudaErrorInvalidValue;
     const unsigned threads = 32u * (unsigned)p->warps;
     if (precision == 0)
-        jac_rows_kernel<double><<<grid, threads, p->smem, s>>>(m, p->lptr, p->lrx, p->lnu, P, T, Y, (double*)J, ng,
-                                                               scratch);
+        jac_rows_kernel<double><<<grid, threads, p->smem, s>>>(m, p->lptr, p->lrx, p->lnu, p->lrow, P, T, Y,
+                                                               (double*)J, ng, scratch);
     else
-        jac_rows_kernel<float><<<grid, threads, p->smem, s>>>(m, p->lptr, p->lrx, p->lnu, P, T, Y, (float*)J, ng,
-                                                              scratch);
+        jac_rows_kernel<float><<<grid, threads, p->smem, s>>>(m, p->lptr, p->lrx, p->lnu, p->lrow, P, T, Y,
+                                                              (float*)J, ng, scratch);
     return cudaGetLastError();
 }
 
