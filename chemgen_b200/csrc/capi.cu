@@ -25,7 +25,8 @@ struct StagedPlan;
 cudaError_t staged_prepare(const DevMech& m, const cg_mech_view& v, int device, StagedPlan** out);
 void staged_release(StagedPlan* p);
 cudaError_t launch_getrates_staged(const StagedPlan* p, const DevMech& m, const double* P, const double* T,
-                                   const double* Y, double* wdot, int64_t ng, cudaStream_t s);
+                                   const double* Y, double* wdot, int64_t ng, cudaStream_t s,
+                                   const unsigned long long* count = nullptr);
 
 struct MixedPlan;
 cudaError_t mixed_prepare(const DevMech& m, const cg_mech_view& v, int device, MixedPlan** out);
@@ -485,19 +486,19 @@ int chemgen_create(const void* blob, size_t nbytes, int device, chemgen_handle**
     h->fp64_block = cg::fp64_smem_block(h->ns, prop.sharedMemPerMultiprocessor, prop.sharedMemPerBlockOptin,
                                         &smem_pts);
     h->fp64_slices = (int64_t)h->sm_count * cg::fp64_global_blocks_per_sm();
-    // Fewer than 8 warps of points per SM in shared memory (state too large
-    // for one thread per point to hide its latencies): the staged kernel when
-    // its tile fits, else the global-scratch kernel (or the low-occupancy
-    // shared-memory kernel, when there is one)
-    if (!h->fp64_block || smem_pts < 256) {
-        e = cg::staged_prepare(h->m, v, device, &h->staged);
-        if (e == cudaSuccess) {
-            h->fp64_block = 0;
-        } else if (e != cudaErrorNotSupported) {
-            cudaFree(h->dbuf);
-            delete h;
-            return status_of(e);
-        }
+    // The staged kernel whenever its tile fits: it is the FP64 kernel when
+    // the one-thread-per-point kernel would hold fewer than 8 warps of points
+    // per SM in shared memory (state too large for one thread per point to
+    // hide its latencies) or none, and it serves the batches whose size is
+    // known only on the device (chemgen_getrates_counted).  Beyond it, the
+    // global-scratch kernel.
+    e = cg::staged_prepare(h->m, v, device, &h->staged);
+    if (e == cudaSuccess) {
+        if (smem_pts < 256) h->fp64_block = 0;
+    } else if (e != cudaErrorNotSupported) {
+        cudaFree(h->dbuf);
+        delete h;
+        return status_of(e);
     }
     e = cg::jac_prepare(h->m, v, device, &h->jac);
     if (e != cudaSuccess && e != cudaErrorNotSupported) {
@@ -601,6 +602,18 @@ int chemgen_getrates_ex(chemgen_handle* h, int mode, const double* P, const doub
 int chemgen_getrates(chemgen_handle* h, const double* P, const double* T, int64_t ng, const double* Y, double* wdot,
                      void* stream) {
     return chemgen_getrates_ex(h, CHEMGEN_MODE_FP64, P, T, ng, Y, wdot, stream);
+}
+
+int chemgen_getrates_counted(chemgen_handle* h, const double* P, const double* T, int64_t ng, const double* Y,
+                             double* wdot, const uint64_t* count, void* stream) {
+    int st = check_args(h, P, T, ng, Y, wdot);
+    if (st || ng == 0) return st;
+    if (!count) return CHEMGEN_ERR_INVALID_ARGUMENT;
+    if (reinterpret_cast<uintptr_t>(count) & 7u) return CHEMGEN_ERR_MISALIGNED;
+    if (!h->staged) return CHEMGEN_ERR_UNSUPPORTED;
+    DeviceGuard g(h->device);
+    return status_of(cg::launch_getrates_staged(h->staged, h->m, P, T, Y, wdot, ng, (cudaStream_t)stream,
+                                                reinterpret_cast<const unsigned long long*>(count)));
 }
 
 int chemgen_workspace_bytes(const chemgen_handle* h, int mode, int64_t ng, size_t* bytes) {

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <utility>
 #include <vector>
 
@@ -939,6 +940,15 @@ cudaError_t launch_jacobian_rows(const JacPlan* p, const DevMech& m, int precisi
     const unsigned grid = (unsigned)std::min<int64_t>(tiles, p->grid);
     if (!scratch || scratch_bytes < jac_rows_workspace_bytes(p, m, ng)) return cudaErrorInvalidValue;
     const unsigned threads = 32u * (unsigned)p->warps;
+    // the kernel's shared-memory limit is this plan's, set under one lock with
+    // the launch (a plan made later for a smaller mechanism sets it lower)
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    cudaError_t e = precision == 0 ? cudaFuncSetAttribute(jac_rows_kernel<double>,
+                                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem)
+                                   : cudaFuncSetAttribute(jac_rows_kernel<float>,
+                                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem);
+    if (e != cudaSuccess) return e;
     if (precision == 0)
         jac_rows_kernel<double><<<grid, threads, p->smem, s>>>(m, p->lptr, p->lrx, p->lnu, p->lrow, P, T, Y,
                                                                (double*)J, ng, scratch);
@@ -984,6 +994,8 @@ cudaError_t launch_vjp(const DevMech& m, const double* P, const double* T, const
     const int w = vjp_tile_warps(m.ns, (size_t)optin);
     if (w >= 4) {
         const size_t smem = (size_t)(4 + w) * m.ns * kJTile * 8 + (size_t)3 * kVMaxWarps * kJTile * 8;
+        static std::mutex mu;
+        std::lock_guard<std::mutex> lk(mu);
         e = cudaFuncSetAttribute(vjp_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         const int64_t tiles = (ng + kJTile - 1) / kJTile;

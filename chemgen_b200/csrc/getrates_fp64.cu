@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <utility>
+#include <mutex>
 #include <vector>
 
 #include "cg_math.cuh"
@@ -434,18 +435,22 @@ __global__ void __launch_bounds__(32 * W, 1)
     getrates_fp64_staged(DevMech m, int R, int nchunk, const int* __restrict__ cptr, const int* __restrict__ cer,
                          const double* __restrict__ cnu, const StFast* __restrict__ fast,
                          const double* __restrict__ P, const double* __restrict__ Tg,
-                         const double* __restrict__ Y, double* __restrict__ wdot, int64_t ng) {
+                         const double* __restrict__ Y, double* __restrict__ wdot, int64_t ng,
+                         const unsigned long long* __restrict__ count) {
     extern __shared__ double smem[];
     const int ns = m.ns;
+    // the arrays' stride is ng; with a device-side count only its first
+    // min(*count, ng) points are computed
+    const int64_t npts = count ? min(ng, (int64_t)*count) : ng;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double* sC = smem;                       // [ns + 1][32] (row ns: the dummy species, 1)
     double* sE = sC + (ns + 1) * kStTile;    // [ns + 1][32]
     double* sQ = sE + (ns + 1) * kStTile;    // [R][32]
     double* sRed = sQ + R * kStTile;         // [W][32]
-    const int64_t ntiles = (ng + kStTile - 1) / kStTile;
+    const int64_t ntiles = (npts + kStTile - 1) / kStTile;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int64_t i = tile * kStTile + lane;
-        const bool act = i < ng;
+        const bool act = i < npts;
         const double T = act ? Tg[i] : 1000.0;
         const double Pp = act ? P[i] : kPatm;
         // ytoc.j2:3-18; species k handled by warp k % W, sums met in shared memory
@@ -713,14 +718,24 @@ void staged_release(StagedPlan* p) {
 }
 
 cudaError_t launch_getrates_staged(const StagedPlan* p, const DevMech& m, const double* P, const double* T,
-                                   const double* Y, double* wdot, int64_t ng, cudaStream_t s) {
+                                   const double* Y, double* wdot, int64_t ng, cudaStream_t s,
+                                   const unsigned long long* count) {
     if (ng <= 0) return cudaSuccess;
     const int64_t tiles = (ng + kStTile - 1) / kStTile;
     const unsigned grid = (unsigned)std::min<int64_t>(tiles, p->grid);
     const unsigned threads = 32u * (unsigned)p->W;
+    // Every plan of the same kernel instance (one per handle) sets the
+    // instance's shared-memory limit to its own size: set it and launch
+    // under one lock, so that a handle made later for a smaller mechanism
+    // cannot leave the limit below this plan's.
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    cudaError_t e = cudaFuncSetAttribute(staged_kernel(p->kpw), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)p->smem);
+    if (e != cudaSuccess) return e;
 #define CG_STAGED_LAUNCH(K)                                                                                  \
     getrates_fp64_staged<16, K><<<grid, threads, p->smem, s>>>(m, p->R, p->nchunk, p->ptr, p->er, p->enu, p->fast, \
-                                                               P, T, Y, wdot, ng)
+                                                               P, T, Y, wdot, ng, count)
     switch (p->kpw) {
         case 8: CG_STAGED_LAUNCH(8); break;
         case 16: CG_STAGED_LAUNCH(16); break;

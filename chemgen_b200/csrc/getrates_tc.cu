@@ -31,6 +31,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "cg_math.cuh"
@@ -782,6 +783,13 @@ cudaError_t launch_getrates_mixed(const MixedPlan* p, const DevMech& m, const do
         if (grid < 1 || !scratch) return cudaErrorInvalidValue;
     }
     double* gs = p->g_smem ? nullptr : (double*)scratch;
+    // the kernel's shared-memory limit is this plan's, set under one lock with
+    // the launch (a plan made later for a smaller mechanism sets it lower)
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    const cudaError_t e = cudaFuncSetAttribute(kernel_for(p->g_smem, p->nt),
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->smem);
+    if (e != cudaSuccess) return e;
     switch ((p->g_smem ? 10 : 0) + p->nt) {
         case 14: return launch_tc<true, 4>(p, m, P, T, Y, wdot, ng, gs, grid, s);
         case 12: return launch_tc<true, 2>(p, m, P, T, Y, wdot, ng, gs, grid, s);

@@ -51,6 +51,7 @@ def lib() -> ctypes.CDLL:
     L.chemgen_num_reactions.argtypes = [vp]
     L.chemgen_getrates.argtypes = [vp, vp, vp, i64, vp, vp, vp]
     L.chemgen_getrates_ex.argtypes = [vp, ci, vp, vp, i64, vp, vp, vp]
+    L.chemgen_getrates_counted.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp]
     L.chemgen_workspace_bytes.argtypes = [vp, ci, i64, ctypes.POINTER(sz)]
     L.chemgen_getrates_ws.argtypes = [vp, ci, vp, vp, i64, vp, vp, vp, sz, vp]
     L.chemgen_getrates_host.argtypes = [vp, ci, vp, vp, i64, vp, vp]
@@ -112,7 +113,8 @@ def lib() -> ctypes.CDLL:
     L.chemgen_kernel_kind.argtypes = [vp, ci]
     L.chemgen_register_kernels.argtypes = [ctypes.c_uint64, ci, ci, ctypes.c_uint, vp]
     for f in ("chemgen_create", "chemgen_destroy", "chemgen_num_species", "chemgen_num_reactions",
-              "chemgen_getrates", "chemgen_getrates_ex", "chemgen_workspace_bytes", "chemgen_getrates_ws",
+              "chemgen_getrates", "chemgen_getrates_ex", "chemgen_getrates_counted", "chemgen_workspace_bytes",
+              "chemgen_getrates_ws",
               "chemgen_getrates_host", "chemgen_init_constants", "chemgen_free_constants",
               "chemgen_init_constants_file", "chemgen_global_num_species",
               "chemgen_last_wrapper_status", "chemgen_use_generated", "chemgen_kernel_kind",

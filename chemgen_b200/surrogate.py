@@ -734,30 +734,52 @@ class SurrogateGetrates:
 
     On CUDA tensors the gate runs on the device behind the fused inference
     kernel, with no host round trip in between: chemgen_gate_select lists the
-    failing points, chemgen_gate_gather packs their states into a batch of
-    `cap` points, the exact kernel runs on that batch and chemgen_gate_scatter
-    writes its results over the surrogate's.  The host reads the count once,
-    at the end of the call; if more points failed than the batch holds, all
-    failing points go through the host path (`_host_gate`) and the batch
-    grows for the next call.  The batch starts at one wave of the exact
-    kernel (65536 points) because an exact launch over fewer points takes
-    about as long: a point's latency, not the batch size, sets its time."""
+    failing points, chemgen_gate_gather packs their states into a batch, the
+    exact kernel runs on that batch and chemgen_gate_scatter writes its
+    results over the surrogate's.  Two ways to run the batch:
+
+    * exact_mode="fp64" (when the mechanism's handle has the staged FP64
+      kernel): the batch holds every point and chemgen_getrates_counted
+      computes only the points counted on the device, so nothing waits for
+      the host; the fallback rate is read when `last_fallback` is asked for.
+      The staged kernel costs ~5x the generated mixed kernel per point, so
+      this suits the few-tenths-of-a-percent fallback of a gate at its
+      tolerance.
+    * otherwise (exact_mode="mixed", or no staged kernel): a batch of `cap`
+      points on the exact kernel of that mode, and one read of the count at
+      the end of the call; if more points failed than the batch holds, all
+      failing points go through the host path (`_host_gate`) and the batch
+      grows for the next call.  The batch starts at one wave of the exact
+      kernel (65536 points) because an exact launch over fewer points takes
+      about as long: a point's latency, not the batch size, sets its time."""
 
     MIN_CAP = 1 << 16
 
-    def __init__(self, sur: Surrogate, tol: float, exact_mode: str = "mixed", margin: float = 0.0,
+    def __init__(self, sur: Surrogate, tol: float, exact_mode: str = "fp64", margin: float = 0.0,
                  cap: int = 0):
         self.sur = sur
         self.tol = tol
         self.exact_mode = exact_mode
         self.margin = margin
-        self.last_fallback = 0.0
+        self._last = 0.0
+        self._pending = None          # (buffers, ng) of a call whose count is still on the device
         self._cap = cap
         self._bufs = None
+        self._counted = exact_mode == "fp64"   # cleared when the handle has no staged kernel
 
     @property
     def threshold(self) -> float:
         return math.log10(self.tol) - self.margin
+
+    @property
+    def last_fallback(self) -> float:
+        """Fraction of the last call's points sent to the exact kernel."""
+        if self._pending is not None:
+            b, ng = self._pending
+            b["done"].synchronize()
+            self._last = int(b["count_host"][0]) / ng
+            self._pending = None
+        return self._last
 
     def _host_gate(self, P, T, Y, W, est):
         """Host-side gate: every failing point through the exact kernel."""
@@ -770,14 +792,14 @@ class SurrogateGetrates:
             W[:, bad] = self.sur.gm.getrates(Pb, Tb, Yb, mode=self.exact_mode)
         return bad.numel()
 
-    def _buffers(self, ng: int):
-        """Batch buffers of the device gate; the unused slots always hold a
-        valid state (1 atm, 1000 K, equal mass fractions, or a state of an
-        earlier call), so the exact kernel's work on them is harmless.  The
-        error-estimate buffer follows ng; device pointers are kept so that a
-        call does little host work between its launches."""
+    def _buffers(self, ng: int, cap: int):
+        """Batch buffers of the device gate (cap points) and the estimate
+        buffer (ng points); device pointers are kept so that a call does
+        little host work between its launches.  On the batch path the unused
+        slots always hold a valid state (1 atm, 1000 K, equal mass fractions,
+        or a state of an earlier call), so the exact kernel's work on them is
+        harmless."""
         import torch
-        cap = min(ng, max(self._cap, self.MIN_CAP))
         b = self._bufs
         if b is None or b["cap"] != cap:
             dev, ns = self.sur.dev, self.sur.ns
@@ -805,25 +827,41 @@ class SurrogateGetrates:
         if not (T.is_cuda and ng):
             # the fused kernel folds the training-support check into the estimate
             W, est = self.sur.predict(P, T, Y, check_range=True)
-            self.last_fallback = self._host_gate(P, T, Y, W, est) / max(ng, 1)
+            self._pending = None
+            self._last = self._host_gate(P, T, Y, W, est) / max(ng, 1)
             if out is not None:
                 out.copy_(W)
                 return out
             return W
-        b = self._buffers(ng)
+        cap = ng if self._counted else min(ng, max(self._cap, self.MIN_CAP))
+        b = self._buffers(ng, cap)
         est = b["est"]
         W = out if out is not None else torch.empty((self.sur.ns, ng), dtype=torch.float64, device=self.sur.dev)
         self.sur.predict_fused(P, T, Y, W, est, check_range=True)
-        cap, ns, s, L = b["cap"], self.sur.ns, _stream(), lib()
+        ns, s, L = self.sur.ns, _stream(), lib()
         check(L.chemgen_gate_select(est.data_ptr(), self.threshold, ng, b["p_idx"], cap, b["p_count"], s),
               "gate_select")
         check(L.chemgen_gate_gather(P.data_ptr(), T.data_ptr(), Y.data_ptr(), ns, ng, b["p_idx"], b["p_count"], cap,
                                     b["p_P"], b["p_T"], b["p_Y"], s), "gate_gather")
-        self.sur.gm.getrates_ptr(b["p_P"], b["p_T"], cap, b["p_Y"], b["p_W"], self.exact_mode, s)
+        if self._counted:
+            st = L.chemgen_getrates_counted(self.sur.gm._h, b["p_P"], b["p_T"], cap, b["p_Y"], b["p_W"],
+                                            b["p_count"], s)
+            if st == 6:                             # no staged kernel for this mechanism: batch path
+                self._counted = False
+                self._bufs = None
+                return self(P, T, Y, out=W)
+            check(st, "chemgen_getrates_counted")
+        else:
+            self.sur.gm.getrates_ptr(b["p_P"], b["p_T"], cap, b["p_Y"], b["p_W"], self.exact_mode, s)
         check(L.chemgen_gate_scatter(b["p_W"], ns, cap, b["p_idx"], b["p_count"], W.data_ptr(), ng, s),
               "gate_scatter")
         b["count_host"].copy_(b["count"], non_blocking=True)
         b["done"].record()
+        if self._counted:
+            # the batch holds every point: nothing can overflow, so the host
+            # reads the count only when the fallback rate is asked for
+            self._pending = (b, ng)
+            return W
         b["done"].synchronize()
         n = int(b["count_host"][0])
         if n > cap:
@@ -831,5 +869,6 @@ class SurrogateGetrates:
             # the host path, and a larger batch next time
             self._host_gate(P, T, Y, W, est)
             self._cap = min(ng, -(-(n + n // 4) // self.MIN_CAP) * self.MIN_CAP)
-        self.last_fallback = n / ng
+        self._pending = None
+        self._last = n / ng
         return W

@@ -69,6 +69,17 @@ int chemgen_getrates(chemgen_handle* h, const double* P, const double* T, int64_
 int chemgen_getrates_ex(chemgen_handle* h, int mode, const double* P, const double* T, int64_t ng,
                         const double* Y, double* wdot, void* stream);
 
+/* FP64 getrates on the first min(*count, ng) points of arrays laid out for ng
+ * points (species stride ng), with `count` a device pointer read by the
+ * kernel (no counterpart in the reference).  For a batch whose size is known
+ * only on the device, such as the points an error gate sends back
+ * (chemgen_gate_select): a launch covers only the points counted, so the
+ * batch can be sized for every point and nothing waits for the host.  Points
+ * past the count are left as they are.  Runs on the staged FP64 kernel;
+ * CHEMGEN_ERR_UNSUPPORTED for a mechanism too large for it.  Asynchronous. */
+int chemgen_getrates_counted(chemgen_handle* h, const double* P, const double* T, int64_t ng, const double* Y,
+                             double* wdot, const uint64_t* count, void* stream);
+
 /* Scratch a call needs for `ng` points in `mode` (0 when the per-point state
  * fits in shared memory), and the variant that uses caller-owned scratch of
  * at least that many bytes (256-byte aligned) instead of library-owned memory. */
@@ -105,14 +116,16 @@ int chemgen_kernel_kind(chemgen_handle* h, int mode);
  *   column c = 0 for T, 1 + j for Y_j; precision 0 = double, 1 = float
  *   (FP64 rate evaluation and accumulation, J stored in FP32).  Each row is
  *   accumulated on chip and J is written once when a 32-point tile's state
- *   and two rows fit in shared memory (up to ~180 species); the tile's rate
- *   constants go to library-owned scratch of 5*nr*32 doubles per SM (about
- *   60 MB at 325 reactions, resident in L2).  Larger mechanisms accumulate J
- *   in place with library-owned scratch of 4*ns*ng doubles (FP32
- *   accumulation for precision 1). 
+ *   and two rows fit in shared memory (up to ~180 species); each tile's
+ *   reaction derivatives or rate constants go to library-owned scratch of
+ *   8*nr*32 doubles per SM (about 100 MB at 325 reactions).  Larger
+ *   mechanisms accumulate J in place with library-owned scratch of 4*ns*ng
+ *   doubles (FP32 accumulation for precision 1).
  * chemgen_getrates_vjp: given G = dL/dwdot [ns*ng], the adjoint
  *   gT = dL/dT [ng], gY = dL/dY [ns*ng] and (if gP != NULL) gP = dL/dP [ng],
- *   without forming J (library-owned scratch of 4*ns*ng doubles). */
+ *   without forming J: up to ~110 species with each 32-point tile's state in
+ *   shared memory and a result that does not depend on scheduling, beyond
+ *   that with library-owned scratch of 4*ns*ng doubles. */
 int chemgen_jacobian(chemgen_handle* h, int precision, const double* P, const double* T, int64_t ng,
                      const double* Y, void* J, void* stream);
 int chemgen_getrates_vjp(chemgen_handle* h, const double* P, const double* T, int64_t ng, const double* Y,

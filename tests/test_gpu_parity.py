@@ -284,3 +284,37 @@ def test_point_major_layout_matches_species_major():
     assert torch.equal(Yp.grad.t(), Ys.grad)
     with pytest.raises(ValueError):
         gm.getrates(P, T, Y, layout="rows")
+
+
+@pytest.mark.parametrize("factory,counts", [(synthetic.h2o2_10sp, [0, 1, 777, 4096, 10 ** 9]),
+                                            (synthetic.gri_shape, [0, 33, 4095, 4096])])
+def test_counted_getrates_computes_only_the_counted_points(factory, counts):
+    """chemgen_getrates_counted: with the count on the device, the first
+    min(count, ng) points equal the staged FP64 kernel's (and the oracle's
+    within the FP64 bar), and the rest of the output is left as it was; a
+    count past ng covers every point."""
+    import torch
+    from chemgen_b200.runtime import lib
+    mech = factory()
+    blob = pack.pack(mech).to_blob()
+    ng = 4096
+    P, T, Y = synthetic.states(mech.ns, ng, seed=17)
+    gm = GpuMechanism(blob)
+    dev = torch.device("cuda", 0)
+    Pt, Tt, Yt = (torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in (P, T, Y))
+    r = oracle.rates(blob, P, T, Y, mech.nr)
+    s = torch.cuda.current_stream().cuda_stream
+    for c in counts:
+        count = torch.tensor([c], dtype=torch.int64, device=dev)
+        W = torch.full((mech.ns, ng), -3.0, dtype=torch.float64, device=dev)
+        assert lib().chemgen_getrates_counted(gm._h, Pt.data_ptr(), Tt.data_ptr(), ng, Yt.data_ptr(), W.data_ptr(),
+                                              count.data_ptr(), s) == 0
+        torch.cuda.synchronize()
+        n = min(c, ng)
+        w = W.cpu().numpy()
+        assert (w[:, n:] == -3.0).all()
+        if n:
+            e = oracle.errors(w[:, :n], r["wdot"][:, :n], r["S"][:, :n])
+            assert e["norm_max"] <= TOL_FP64, e
+    assert lib().chemgen_getrates_counted(gm._h, Pt.data_ptr(), Tt.data_ptr(), ng, Yt.data_ptr(), W.data_ptr(),
+                                          0, s) == 1

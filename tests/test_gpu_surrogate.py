@@ -531,12 +531,19 @@ def test_gate_kernels_select_gather_scatter(ng, cap):
                                       ng, s) == 1
 
 
-def test_device_gate_matches_host_gate(small_surrogate):
+@pytest.mark.parametrize("exact_mode", ["fp64", "mixed"])
+def test_device_gate_matches_host_gate(small_surrogate, exact_mode):
     """The device-side gate (no host round trip between the fused kernel and
-    the exact one) gives bit for bit what the host-side gate gives, with the
-    batch large enough, with more failing points than the batch holds (the
-    call then finishes on the host path and grows the batch) and again after
-    that growth; the fallback rate is the count of failing points."""
+    the exact one) gives what the host-side gate gives: bit for bit with
+    exact_mode "mixed"; with "fp64" bit for bit on the trusted points and
+    within 1e-12 on the points sent back (the host gate's FP64 call may run
+    the generated FP64 kernel, the counted batch the staged one).  With
+    exact_mode "fp64" the batch holds every point and the staged kernel
+    computes only the points counted on the device (the host never waits);
+    with "mixed" the batch has a capacity: large enough, smaller than the
+    failing points (the call then finishes on the host path and grows the
+    batch), and again after that growth.  Two calls in a row; the fallback
+    rate is the count of failing points."""
     import torch
     from chemgen_b200 import surrogate as S
     sur = small_surrogate
@@ -545,16 +552,28 @@ def test_device_gate_matches_host_gate(small_surrogate):
     W0, est = sur.predict(P, T, Y, check_range=True)
     for q in (0.02, 0.6):               # 2 % and 60 % of the points fail
         tol = 10 ** float(torch.quantile(est.double(), 1.0 - q))
-        host = S.SurrogateGetrates(sur, tol=tol)
+        host = S.SurrogateGetrates(sur, tol=tol, exact_mode=exact_mode)
         Wh, eh = sur.predict(P, T, Y, check_range=True)
         nh = host._host_gate(P, T, Y, Wh, eh)
-        dev = S.SurrogateGetrates(sur, tol=tol)
+        dev = S.SurrogateGetrates(sur, tol=tol, exact_mode=exact_mode)
+        Wd = torch.empty_like(Wh)
+        back = ~(eh <= dev.threshold)
         for call in range(2):
-            Wd = dev(P, T, Y)
+            dev(P, T, Y, out=Wd)
             torch.cuda.synchronize()
-            assert torch.equal(Wd, Wh), (q, call)
+            if exact_mode == "mixed":
+                assert torch.equal(Wd, Wh), (exact_mode, q, call)
+            else:
+                # the host gate's FP64 call may run the mechanism's generated
+                # FP64 kernel (when another test loaded it), the counted batch
+                # the staged one: the same arithmetic in another order
+                assert torch.equal(Wd[:, ~back], Wh[:, ~back]), (exact_mode, q, call)
+                rel = ((Wd - Wh).abs().max(0).values / Wh.abs().max(0).values.clamp_min(1e-300)).max().item()
+                assert rel < 1e-12, (exact_mode, q, call, rel)
             assert dev.last_fallback == pytest.approx(nh / ng)
-        if q > 0.5:
+        if exact_mode == "fp64":
+            assert dev._counted and dev._bufs["cap"] == ng
+        elif q > 0.5:
             assert dev._bufs["cap"] >= nh          # grown after the first call's overflow
         else:
             assert dev._bufs["cap"] == dev.MIN_CAP
