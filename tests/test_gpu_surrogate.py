@@ -317,13 +317,12 @@ def test_surrogate_trains_and_gains_over_exact_kernel():
 
 def test_gated_surrogate_gain_and_leakage():
     """With the bench's training (10^7 samples, 16 epochs) and its 5 %
-    tolerance, the gated surrogate (fused inference, exact mixed kernel for
-    the points the gate sends back) is faster than the FP64 kernel on all
-    points, and the error left after the gate is bounded at the 99.9th
-    percentile; the strict gate (margin 0.5) trades fallback for accuracy.
-    Against the mixed kernel the times are printed: since the generated
-    kernels' streaming cache hints and 16-warp mixed form, the mixed kernel
-    (~1050 Mpts/s at 2^22 points) outruns the fused inference (~900)."""
+    tolerance, the gated surrogate (fused inference, the counted FP64 batch
+    for the points the gate sends back) is faster than the FP64 kernel and
+    than the mixed kernel on all points (on B200 at 2^22 points: ~3.75 ms
+    against ~5.8 and ~3.9 ms), and the error left after the gate is bounded
+    at the 99.9th percentile; the strict gate (margin 0.5) trades fallback
+    for accuracy."""
     import torch
     from chemgen_b200 import surrogate as S
     gm = GpuMechanism(synthetic.gri_shape(), generated=True)
@@ -347,19 +346,22 @@ def test_gated_surrogate_gain_and_leakage():
         return a.elapsed_time(b) / reps
 
     t_fp64, t_mixed, t_gate = [], [], []
+    Wg = torch.empty_like(W64)
     for _ in range(3):        # interleaved, best of three each
         t_fp64.append(ms(lambda: gm.getrates(P, T, Y, out=W, mode="fp64")))
         t_mixed.append(ms(lambda: gm.getrates(P, T, Y, out=W, mode="mixed")))
-        t_gate.append(ms(lambda: run(P, T, Y)))
+        t_gate.append(ms(lambda: run(P, T, Y, out=Wg)))
     nerr = lambda X: ((X - W64).abs().max(dim=0).values / W64.abs().max(dim=0).values).cpu().numpy()
     e = nerr(run(P, T, Y))
-    strict = S.SurrogateGetrates(sur, tol=0.05, margin=0.5)
+    # the strict gate sends back ~6 %: the mixed kernel's fixed batch, as in the bench
+    strict = S.SurrogateGetrates(sur, tol=0.05, margin=0.5, exact_mode="mixed")
     e_s = nerr(strict(P, T, Y))
     print(info, "fp64 ms", t_fp64, "mixed ms", t_mixed, "gated ms", t_gate, "fallback", run.last_fallback,
           strict.last_fallback, "after gate p99.9 / max", np.quantile(e, 0.999), e.max(), "strict",
           np.quantile(e_s, 0.999), e_s.max())
     assert run.last_fallback < 0.01
     assert min(t_gate) < min(t_fp64)
+    assert min(t_gate) < min(t_mixed)
     assert np.quantile(e, 0.999) < 0.15
     assert strict.last_fallback > run.last_fallback and np.quantile(e_s, 0.999) <= np.quantile(e, 0.999)
 
