@@ -834,6 +834,9 @@ class SurrogateGetrates:
                 return out
             return W
         cap = ng if self._counted else min(ng, max(self._cap, self.MIN_CAP))
+        if out is not None and not (out.is_cuda and out.dtype == torch.float64 and out.is_contiguous()
+                                    and tuple(out.shape) == (self.sur.ns, ng)):
+            raise ValueError(f"out must be a contiguous float64 CUDA tensor of shape ({self.sur.ns}, {ng})")
         b = self._buffers(ng, cap)
         est = b["est"]
         W = out if out is not None else torch.empty((self.sur.ns, ng), dtype=torch.float64, device=self.sur.dev)
