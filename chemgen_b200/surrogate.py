@@ -744,7 +744,8 @@ class SurrogateGetrates:
       the host; the fallback rate is read when `last_fallback` is asked for.
       The staged kernel costs ~5x the generated mixed kernel per point, so
       this suits the few-tenths-of-a-percent fallback of a gate at its
-      tolerance.
+      tolerance.  The batch buffers hold 2 ns + 3 values per point (a copy
+      of the states and rates of every point, on the device).
     * otherwise (exact_mode="mixed", or no staged kernel): a batch of `cap`
       points on the exact kernel of that mode, and one read of the count at
       the end of the call; if more points failed than the batch holds, all
