@@ -772,6 +772,13 @@ class SurrogateGetrates:
     def threshold(self) -> float:
         return math.log10(self.tol) - self.margin
 
+    @classmethod
+    def grown_cap(cls, n: int, ng: int) -> int:
+        """Batch capacity after a call in which n of ng points failed and
+        overflowed the batch: a quarter more than n, in whole multiples of
+        MIN_CAP, at most ng."""
+        return min(ng, -(-(n + n // 4) // cls.MIN_CAP) * cls.MIN_CAP)
+
     @property
     def last_fallback(self) -> float:
         """Fraction of the last call's points sent to the exact kernel."""
@@ -872,7 +879,7 @@ class SurrogateGetrates:
             # more failing points than the batch holds: all of them through
             # the host path, and a larger batch next time
             self._host_gate(P, T, Y, W, est)
-            self._cap = min(ng, -(-(n + n // 4) // self.MIN_CAP) * self.MIN_CAP)
+            self._cap = self.grown_cap(n, ng)
         self._pending = None
         self._last = n / ng
         return W

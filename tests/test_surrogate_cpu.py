@@ -99,3 +99,16 @@ def test_no_fallback_call_when_all_trusted():
     run = S.SurrogateGetrates(sur, tol=1e-3)
     run(torch.full_like(T, 1013250.0), T, torch.full((2, 2), 0.5, dtype=torch.float64))
     assert sur.gm.calls == [] and run.last_fallback == 0.0
+
+
+def test_gate_batch_growth_rule():
+    """After an overflow the fixed batch grows to a quarter more than the
+    failing points, in whole multiples of one wave (65536), never past ng."""
+    g = S.SurrogateGetrates.grown_cap
+    m = S.SurrogateGetrates.MIN_CAP
+    assert m == 65536
+    assert g(70000, 1 << 22) == 2 * m            # 87500 -> two waves
+    assert g(4 * m, 1 << 22) == 5 * m            # 327680 exactly
+    assert g(4 * m + 4, 1 << 22) == 6 * m
+    assert g(200000, 150000) == 150000           # capped at ng
+    assert g(1, 1 << 22) == m
